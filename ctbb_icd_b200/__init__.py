@@ -1,0 +1,383 @@
+"""B200-native reconstruction path for CTBB_ICD.
+
+Python mirror of the reference program's stage functions (src/main.cpp:88-128):
+
+    rp   = configure_recon_params(prm_path)          # setup.cpp:69
+    data = load_raw(rp)                              # setup.cpp:245
+    initialize_recon_volume(rp, data)                # initialize_recon_volume.cpp:51
+    generate_system_matrix(rp, data)                 # generate_system_matrix[_ffs].cpp
+    icd_iteration(rp, data)                          # icd_iteration.cpp:42
+    rotate_slices_rotating2fixed(rp, data)           # rotate_slices.cpp:81
+    clean_up(rp, data)                               # setup.cpp:422
+
+Same argument meaning as the reference; errors raise CtbbError (the
+reference printed a message and exited). All numerical work runs in the CUDA
+kernels of libctbb_icd_b200.so; there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from ._lib import (  # noqa: F401
+    ICD_GROUPED, ICD_SEQUENTIAL, PENALTY_EDGE_PRESERVING, PENALTY_QUADRATIC,
+    ROTATE_FIXED2ROTATING, ROTATE_ROTATING2FIXED, SSM_BOTH, SSM_FP16, SSM_FP32, CtbbError,
+    GeomC, IcdOpts, IterStats, PhantomSpec, PrmStrings, SsmInfo, check, lib, ptr,
+)
+
+__all__ = [
+    "ReconParams", "CtData", "Context", "Ssm", "Recon", "CtbbError",
+    "configure_recon_params", "load_raw", "initialize_recon_volume", "generate_system_matrix",
+    "generate_system_matrix_ffs", "icd_iteration", "rotate_slices_rotating2fixed",
+    "rotate_slices_fixed2rotating", "clean_up", "synth_raw_host", "write_raw_file",
+    "slice_tables", "icd_opts",
+]
+
+
+@dataclass
+class ReconParams:
+    """recon_params: numeric fields in `geom` (ctbb_geom_c), strings beside it."""
+
+    geom: GeomC
+    initial_recon_path: str = ""
+    matrix_path: str = ""
+    output_dir: str = ""
+    output_file: str = ""
+    potential: str = ""
+    recon_path: str = ""
+    sinogram_path: str = ""
+    penalty: str = "quadratic"
+
+    def __getattr__(self, name):
+        geom = self.__dict__.get("geom")
+        if geom is not None and name != "geom":
+            key = "lambda_" if name == "lambda" else name
+            return getattr(geom, key)
+        raise AttributeError(name)
+
+    @property
+    def shape(self):
+        g = self.geom
+        return (int(g.num_voxels_z), int(g.num_voxels_y), int(g.num_voxels_x))
+
+    @property
+    def raw_shape(self):
+        g = self.geom
+        return (int(g.Readings), int(g.n_channels), int(g.Nrows_projection))
+
+
+@dataclass
+class CtData:
+    """ct_data (recon_structs.h:116-125) as numpy arrays."""
+
+    raw: np.ndarray | None = None             # float32 [Readings][n_channels][Nrows]
+    recon_volume: np.ndarray | None = None    # float32 [nz][ny][nx]
+    tube_angles: np.ndarray | None = None     # float64 degrees [Readings]
+    table_positions: np.ndarray | None = None  # float64 cm [Readings]
+    slice_locations: np.ndarray | None = None  # float64 cm [nz]
+    slice_indices: np.ndarray | None = None    # uint64 [nz]
+    system_matrix: "Ssm | None" = None         # device-resident SSM
+    extra: dict = field(default_factory=dict)
+
+
+def configure_recon_params(prm_path: str) -> ReconParams:
+    """setup.cpp:69-243: parse, check required fields, apply defaults, derive."""
+    g, s = GeomC(), PrmStrings()
+    check(lib().ctbb_configure_recon_params(str(prm_path).encode(), C.byref(g), C.byref(s)))
+    dec = lambda b: b.decode()  # noqa: E731
+    return ReconParams(
+        geom=g, initial_recon_path=dec(s.initial_recon_path), matrix_path=dec(s.matrix_path),
+        output_dir=dec(s.output_dir), output_file=dec(s.output_file), potential=dec(s.potential),
+        recon_path=dec(s.recon_path), sinogram_path=dec(s.sinogram_path), penalty=dec(s.penalty))
+
+
+def slice_tables(rp: ReconParams, *, allow_bad_range: bool = False) -> CtData:
+    """Tube angles, table positions and rotating-slice tables (setup.cpp:273-409)."""
+    g = rp.geom
+    n = int(g.Readings)
+    ta = np.zeros(n, np.float64)
+    tp = np.zeros(n, np.float64)
+    cap = max(1, int(abs(g.z_end - g.z_start) / g.voxel_size_z) + 2)
+    sl = np.zeros(cap, np.float64)
+    si = np.zeros(cap, np.uint64)
+    st = lib().ctbb_slice_tables(C.byref(g), ptr(ta, C.c_double), ptr(tp, C.c_double),
+                                 ptr(sl, C.c_double), ptr(si, C.c_uint64), cap)
+    if not (allow_bad_range and st == 4):
+        check(st)
+    nz = int(g.num_voxels_z)
+    return CtData(tube_angles=ta, table_positions=tp, slice_locations=sl[:nz].copy(),
+                  slice_indices=si[:nz].copy())
+
+
+def load_raw(rp: ReconParams, *, raw: np.ndarray | None = None) -> CtData:
+    """setup.cpp:245-420 for FileType 0; `raw` bypasses the file read."""
+    data = slice_tables(rp)
+    if raw is None:
+        if not os.path.exists(rp.sinogram_path):
+            raise CtbbError(3, f"Raw data file not found: {rp.sinogram_path}")
+        raw = np.empty(rp.raw_shape, np.float32)
+        check(lib().ctbb_read_raw(rp.sinogram_path.encode(), C.byref(rp.geom), ptr(raw, C.c_float)))
+    data.raw = np.ascontiguousarray(raw, dtype=np.float32).reshape(rp.raw_shape)
+    data.recon_volume = np.zeros(rp.shape, np.float32)
+    return data
+
+
+def initialize_recon_volume(rp: ReconParams, data: CtData) -> None:
+    """initialize_recon_volume.cpp:51-184: zeros, or a float32 volume from
+    initial_recon_path. The wFBP path needs the external ctbb_recon program,
+    which is not part of this build."""
+    if rp.initial_recon_path:
+        if not os.path.exists(rp.initial_recon_path):
+            raise CtbbError(3, "Specified initial reconstruction file not found")
+        vol = np.fromfile(rp.initial_recon_path, np.float32)
+        if vol.size < int(np.prod(rp.shape)):
+            raise CtbbError(3, "Could not initialize reconstruction volume from given file")
+        data.recon_volume = vol[: int(np.prod(rp.shape))].reshape(rp.shape).copy()
+    elif int(rp.geom.wfbp_initialize) != 0:
+        raise CtbbError(9, "wFBP initialisation needs the external ctbb_recon program")
+    else:
+        data.recon_volume = np.zeros(rp.shape, np.float32)
+
+
+def synth_raw_host(rp: ReconParams, phantom: dict, n_threads: int = 1) -> np.ndarray:
+    """Seeded synthetic raw frames on the CPU (stands in for ctbb_read)."""
+    from .workloads import phantom_spec
+
+    g = GeomC.from_buffer_copy(rp.geom)
+    slice_tables(ReconParams(geom=g), allow_bad_range=True)  # sets z_first_view, table_direction
+    spec = phantom_spec(phantom)
+    raw = np.empty(rp.raw_shape, np.float32)
+    check(lib().ctbb_synth_raw_host(C.byref(g), C.byref(spec), ptr(raw, C.c_float), int(n_threads)))
+    return raw
+
+
+def write_raw_file(path: str, rp: ReconParams, raw: np.ndarray) -> None:
+    raw = np.ascontiguousarray(raw, dtype=np.float32)
+    check(lib().ctbb_write_raw_file(str(path).encode(), C.byref(rp.geom), ptr(raw, C.c_float)))
+
+
+# --------------------------------------------------------------------------
+# GPU objects
+# --------------------------------------------------------------------------
+class Context:
+    """One CUDA device + stream (ctbb_gpu_init)."""
+
+    def __init__(self, device: int = 0, stream=None):
+        h = C.c_void_p()
+        check(lib().ctbb_gpu_init(int(device), stream, C.byref(h)))
+        self.handle = h
+
+    @property
+    def stream(self) -> int:
+        return lib().ctbb_gpu_stream(self.handle) or 0
+
+    def synchronize(self):
+        check(lib().ctbb_gpu_synchronize(self.handle))
+
+    def close(self):
+        if self.handle:
+            lib().ctbb_gpu_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+_default_ctx: Context | None = None
+
+
+def default_context() -> Context:
+    global _default_ctx
+    if _default_ctx is None:
+        _default_ctx = Context(0)
+    return _default_ctx
+
+
+class Ssm:
+    """Device-resident stored system matrix."""
+
+    def __init__(self, handle, ctx: Context):
+        self.handle, self.ctx = handle, ctx
+
+    @classmethod
+    def generate(cls, rp: ReconParams, ctx: Context | None = None, weights: int = SSM_BOTH):
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().ctbb_gpu_generate_ssm(ctx.handle, C.byref(rp.geom), int(weights), C.byref(h)))
+        return cls(h, ctx)
+
+    @classmethod
+    def import_reference(cls, rp: ReconParams, path: str, ctx: Context | None = None,
+                         weights: int = SSM_BOTH):
+        ctx = ctx or default_context()
+        h = C.c_void_p()
+        check(lib().ctbb_gpu_ssm_import_reference(ctx.handle, C.byref(rp.geom), str(path).encode(),
+                                                  int(weights), C.byref(h)))
+        return cls(h, ctx)
+
+    def info(self) -> SsmInfo:
+        i = SsmInfo()
+        check(lib().ctbb_gpu_ssm_info(self.handle, C.byref(i)))
+        return i
+
+    def column(self, c: int):
+        n = C.c_uint64()
+        check(lib().ctbb_gpu_ssm_column(self.handle, int(c), None, None, 0, C.byref(n)))
+        idx = np.empty(n.value, np.int32)
+        w = np.empty(n.value, np.float32)
+        check(lib().ctbb_gpu_ssm_column(self.handle, int(c), ptr(idx, C.c_int32), ptr(w, C.c_float),
+                                        n.value, C.byref(n)))
+        return idx, w
+
+    def export_reference(self, path: str):
+        check(lib().ctbb_gpu_ssm_export_reference(self.handle, str(path).encode()))
+
+    def free(self):
+        if self.handle:
+            lib().ctbb_gpu_ssm_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
+             compute_cost=False, stop_rel_change=0.0) -> IcdOpts:
+    o = IcdOpts()
+    o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
+    o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
+    o.compute_cost, o.stop_rel_change = int(bool(compute_cost)), float(stop_rel_change)
+    return o
+
+
+class Recon:
+    """Device-resident ICD state (raw y, image x, error sinogram e)."""
+
+    def __init__(self, rp: ReconParams, slice_indices: np.ndarray, ctx: Context | None = None):
+        self.ctx = ctx or default_context()
+        self.rp = rp
+        self.slice_indices = np.ascontiguousarray(slice_indices, dtype=np.uint64)
+        h = C.c_void_p()
+        check(lib().ctbb_gpu_recon_create(self.ctx.handle, C.byref(rp.geom),
+                                          ptr(self.slice_indices, C.c_uint64), C.byref(h)))
+        self.handle = h
+
+    def set_raw(self, raw: np.ndarray):
+        raw = np.ascontiguousarray(raw, dtype=np.float32)
+        check(lib().ctbb_gpu_recon_set_raw(self.handle, ptr(raw, C.c_float)))
+
+    def set_raw_device(self, dev_ptr: int):
+        check(lib().ctbb_gpu_recon_set_raw_device(self.handle, C.c_void_p(dev_ptr)))
+
+    def raw_device_ptr(self) -> int:
+        return lib().ctbb_gpu_recon_raw_device(self.handle) or 0
+
+    def set_volume(self, ssm: Ssm, vol: np.ndarray | None = None):
+        v = None if vol is None else np.ascontiguousarray(vol, dtype=np.float32)
+        check(lib().ctbb_gpu_recon_set_volume(self.handle, ssm.handle, ptr(v, C.c_float)))
+
+    def volume(self) -> np.ndarray:
+        out = np.empty(self.rp.shape, np.float32)
+        check(lib().ctbb_gpu_recon_get_volume(self.handle, ptr(out, C.c_float)))
+        return out
+
+    def volume_f64(self) -> np.ndarray:
+        out = np.empty(self.rp.shape, np.float64)
+        check(lib().ctbb_gpu_recon_get_volume_f64(self.handle, ptr(out, C.c_double)))
+        return out
+
+    def iterate(self, ssm: Ssm, n_iter: int, opts: IcdOpts | None = None) -> IterStats:
+        st = IterStats()
+        o = opts or icd_opts()
+        check(lib().ctbb_gpu_recon_iterate(self.handle, ssm.handle, C.byref(o), int(n_iter), C.byref(st)))
+        return st
+
+    def refresh_residual(self, ssm: Ssm):
+        check(lib().ctbb_gpu_recon_refresh_residual(self.handle, ssm.handle))
+
+    def cost(self) -> float:
+        c = C.c_double()
+        check(lib().ctbb_gpu_recon_cost(self.handle, C.byref(c)))
+        return c.value
+
+    def free(self):
+        if self.handle:
+            lib().ctbb_gpu_recon_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# Stage functions with the reference's names
+# --------------------------------------------------------------------------
+def generate_system_matrix(rp: ReconParams, data: CtData, ctx: Context | None = None,
+                           weights: int = SSM_BOTH) -> Ssm:
+    """generate_system_matrix.cpp:54 / generate_system_matrix_ffs.cpp:60 on the GPU.
+    The in-plane FFS model is selected from rp.Phiffs, as main.cpp:103-109 does."""
+    data.system_matrix = Ssm.generate(rp, ctx, weights)
+    return data.system_matrix
+
+
+generate_system_matrix_ffs = generate_system_matrix
+
+
+def icd_iteration(rp: ReconParams, data: CtData, ctx: Context | None = None,
+                  opts: IcdOpts | None = None, n_iter: int | None = None) -> IterStats:
+    """icd_iteration.cpp:42-286: num_iterations ICD passes; data.recon_volume in/out."""
+    if data.system_matrix is None:
+        raise CtbbError(1, "generate_system_matrix must run before icd_iteration")
+    ctx = ctx or data.system_matrix.ctx
+    rc = Recon(rp, data.slice_indices, ctx)
+    try:
+        rc.set_raw(data.raw)
+        rc.set_volume(data.system_matrix, data.recon_volume)
+        st = rc.iterate(data.system_matrix, int(n_iter if n_iter is not None else rp.geom.num_iterations),
+                        opts or icd_opts(mode=ICD_SEQUENTIAL))
+        data.recon_volume = rc.volume()
+        data.extra["volume_f64"] = rc.volume_f64()
+    finally:
+        rc.free()
+    return st
+
+
+def _rotate(rp: ReconParams, data: CtData, direction: int, ctx: Context | None):
+    ctx = ctx or default_context()
+    vol = np.ascontiguousarray(data.recon_volume, dtype=np.float32).copy()
+    check(lib().ctbb_gpu_rotate(ctx.handle, C.byref(rp.geom), ptr(data.tube_angles, C.c_double),
+                                ptr(data.slice_indices, C.c_uint64), ptr(vol, C.c_float), int(direction)))
+    data.recon_volume = vol
+
+
+def rotate_slices_rotating2fixed(rp: ReconParams, data: CtData, ctx: Context | None = None):
+    """rotate_slices.cpp:81-114 on the GPU."""
+    _rotate(rp, data, ROTATE_ROTATING2FIXED, ctx)
+
+
+def rotate_slices_fixed2rotating(rp: ReconParams, data: CtData, ctx: Context | None = None):
+    """rotate_slices.cpp:48-79 on the GPU."""
+    _rotate(rp, data, ROTATE_FIXED2ROTATING, ctx)
+
+
+def clean_up(rp: ReconParams, data: CtData) -> str:
+    """setup.cpp:422-438: write the float32 volume to output_dir/output_file."""
+    name = rp.output_file or "reconstruction_final.img"
+    path = os.path.join(rp.output_dir, name)
+    np.ascontiguousarray(data.recon_volume, dtype=np.float32).tofile(path)
+    if data.system_matrix is not None:
+        data.system_matrix.free()
+        data.system_matrix = None
+    return path

@@ -1,0 +1,99 @@
+// Device-resident objects behind the opaque handles of the C ABI, and the
+// internal launch functions shared between translation units.
+#pragma once
+
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.h"
+
+#define CTBB_CUDA(call)                                                                        \
+    do {                                                                                       \
+        cudaError_t err__ = (call);                                                            \
+        if (err__ != cudaSuccess)                                                              \
+            return ::ctbb::fail(err__ == cudaErrorMemoryAllocation ? CTBB_ERR_OOM : CTBB_ERR_CUDA, \
+                                "%s:%d %s: %s", __FILE__, __LINE__, #call,                     \
+                                cudaGetErrorString(err__));                                    \
+    } while (0)
+
+#define CTBB_TRY(call)                        \
+    do {                                      \
+        ctbb_status st__ = (call);            \
+        if (st__ != CTBB_OK) return st__;     \
+    } while (0)
+
+struct ctbb_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int sm_count = 148;
+    size_t smem_per_block_optin = 0;
+    // Reusable FP64 reduction scratch (partial sums), sized on demand.
+    double* d_partials = nullptr;
+    size_t partials_cap = 0;
+    // Work-queue head for the grouped ICD kernel.
+    unsigned long long* d_queue = nullptr;
+    int* d_flags = nullptr;  // device-side error flags
+};
+
+// Stored system matrix: per voxel column c = i + nx*j, entries sorted by
+// q = row + Nrows*(channel + n_channels*view). colptr[c] is the first entry of
+// column c; vptr[c*(nvsm+1) + v] is the offset (relative to colptr[c]) of the
+// first entry of SSM view v, so a view window [v0, v1) is one contiguous run.
+struct ctbb_ssm {
+    ctbb_ctx* ctx = nullptr;
+    ctbb_geom_c geom{};
+    uint64_t ncol = 0, nvsm = 0, nnz = 0, max_col_nnz = 0;
+    int64_t* d_colptr = nullptr;  // [ncol + 1]
+    uint32_t* d_vptr = nullptr;   // [ncol * (nvsm + 1)]
+    int32_t* d_idx = nullptr;     // [nnz]
+    float* d_w32 = nullptr;       // [nnz] (CTBB_SSM_FP32 held)
+    __half* d_w16 = nullptr;      // [nnz] (CTBB_SSM_FP16 held)
+    int weights = 0;
+    int ffs = 0;
+    double build_ms = 0.0;
+    uint64_t bytes = 0;
+};
+
+// Device-resident ICD state. The sequential (parity) mode keeps the image
+// and the sinogram estimate y_hat = A x in FP64 like icd_iteration.cpp:47-48;
+// the grouped mode keeps an FP32 image and the FP32 error sinogram e = y - A x.
+struct ctbb_recon {
+    ctbb_ctx* ctx = nullptr;
+    ctbb_geom_c geom{};
+    uint64_t nvox = 0, data_size = 0;
+    std::vector<uint64_t> slice_indices;
+    int32_t* d_start = nullptr;  // [nz] first data view of each slice's SSM window
+    float* d_raw = nullptr;      // y
+    double* d_x64 = nullptr;     // sequential-mode image
+    double* d_est64 = nullptr;   // sequential-mode A x (FP64); also FP64 refresh accumulator
+    float* d_x32 = nullptr;      // grouped-mode image
+    float* d_e32 = nullptr;      // grouped-mode y - A x
+    int rep = 0;                 // 0: x64/est64 current, 1: x32/e32 current
+};
+
+namespace ctbb {
+
+ctbb_status ensure_partials(ctbb_ctx* ctx, size_t n);
+
+// ssm.cu
+ctbb_status ssm_validate_geometry(const ctbb_geom_c& g);
+
+// recon.cu
+ctbb_status recon_to_grouped(ctbb_recon* rc, const ctbb_ssm* ssm);
+ctbb_status recon_to_sequential(ctbb_recon* rc, const ctbb_ssm* ssm);
+ctbb_status forward_project_f64(ctbb_recon* rc, const ctbb_ssm* ssm, bool from_x32, double* d_out);
+ctbb_status cost_f64(ctbb_recon* rc, const ctbb_ssm* ssm, bool exact, double* out);
+
+// icd_seq.cu
+ctbb_status launch_icd_sequential(ctbb_recon* rc, const ctbb_ssm* ssm, int n_iter, float* ms);
+
+// icd_grouped.cu
+ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o,
+                               float* ms, double* entries);
+int default_warps_in_flight(const ctbb_recon* rc);
+
+}  // namespace ctbb

@@ -1,0 +1,139 @@
+// Slice rotation between the rotating ICD frame and the fixed frame.
+//
+// Replaces rotate_slices_rotating2fixed (rotate_slices.cpp:81-114),
+// rotate_slices_fixed2rotating (:48-79), rotate_slice (:116-154) and interp2
+// (interp.h:41-76). One thread per output pixel gathers its four bilinear
+// taps (an L2-resident slice of at most 1 MB at 512 x 512); the kernel is a
+// pure streaming gather, bounded by HBM bandwidth.
+//
+// Compiled with -fmad=false. The per-slice cos/sin are computed on the host
+// with the reference's expressions, the rotated coordinates in double and
+// rounded to float exactly where rotate_slice.cpp:142-151 rounds them, and
+// the interpolation in float with the reference's operation order, so the
+// output matches the reference bit for bit.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gpu_internal.h"
+
+namespace {
+
+__global__ void __launch_bounds__(256) rotate_kernel(const float* __restrict__ in, float* __restrict__ out, int nx,
+                                                     int ny, int nz, int dim1, int dim2, int out_stride_y,
+                                                     const double* __restrict__ cs, double cvx, double cvy) {
+    const uint64_t npix = (uint64_t)nx * ny;
+    const uint64_t n = npix * nz;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t / npix);
+        const uint64_t p = t % npix;
+        const int x_idx = (int)(p % nx), y_idx = (int)(p / nx);
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        const double x = x_idx - cvx, y = y_idx - cvy;
+        const float xp = (float)(c * x - s * y);
+        const float yp = (float)(s * x + c * y);
+        const float i1 = (float)((double)xp + cvx);
+        const float i2 = (float)((double)yp + cvy);
+        const float* a = in + (uint64_t)k * npix;
+        float val;
+        if (i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0)) {
+            val = 0.0f;
+        } else {
+            const float v = i1 - floorf(i1);
+            const float w = i2 - floorf(i2);
+            const int f1 = (int)floorf(i1), f2 = (int)floorf(i2);
+            const int a1 = f2 * dim1 + f1;
+            const int a2 = f2 * dim1 + f1 + 1;
+            const int a3 = (f2 + 1) * dim1 + f1;
+            const int a4 = (f2 + 1) * dim1 + f1 + 1;
+            val = a[a1] * (1.0f - v) * (1.0f - w) + a[a2] * v * (1.0f - w) + a[a3] * (1.0f - v) * w +
+                  a[a4] * v * w;
+        }
+        // rotate_slices.cpp:128 writes with stride num_voxels_y.
+        out[(uint64_t)k * npix + (uint64_t)x_idx + (uint64_t)y_idx * out_stride_y] = val;
+    }
+}
+
+ctbb_status angles(const ctbb_geom_c& g, const double* tube_angles_deg, const uint64_t* slice_indices, int direction,
+                   std::vector<double>& cs) {
+    const double PI = 3.141592653589793238;  // rotate_slices.cpp:29
+    cs.resize(2 * g.num_voxels_z);
+    for (uint64_t k = 0; k < g.num_voxels_z; ++k) {
+        if (slice_indices[k] >= g.Readings) return ctbb::fail(CTBB_ERR_INVALID_ARG, "slice index out of range");
+        double a = -(tube_angles_deg[slice_indices[k]]) * 2.0 * PI / 360.0;
+        if (direction == CTBB_ROTATE_FIXED2ROTATING) a = -a;
+        cs[2 * k] = cos(a);
+        cs[2 * k + 1] = sin(a);
+    }
+    return CTBB_OK;
+}
+
+ctbb_status rotate_device(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tube_angles_deg,
+                          const uint64_t* slice_indices, const float* d_in, float* d_out, int direction) {
+    using namespace ctbb;
+    if (direction != CTBB_ROTATE_FIXED2ROTATING && direction != CTBB_ROTATE_ROTATING2FIXED)
+        return fail(CTBB_ERR_INVALID_ARG, "direction must be +1 or -1");
+    if (g.num_voxels_x != g.num_voxels_y)
+        return fail(CTBB_ERR_INVALID_ARG, "slice rotation needs square slices (rotate_slices.cpp:128)");
+    std::vector<double> cs;
+    CTBB_TRY(angles(g, tube_angles_deg, slice_indices, direction, cs));
+    double* d_cs = nullptr;
+    CTBB_CUDA(cudaMalloc(&d_cs, cs.size() * sizeof(double)));
+    cudaStream_t st = ctx->stream;
+    cudaError_t e = cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const uint64_t n = g.num_voxels_x * g.num_voxels_y * g.num_voxels_z;
+        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
+        rotate_kernel<<<grid, 256, 0, st>>>(d_in, d_out, (int)g.num_voxels_x, (int)g.num_voxels_y,
+                                            (int)g.num_voxels_z, (int)g.nx, (int)g.ny, (int)g.num_voxels_y, d_cs,
+                                            g.center_voxel_x, g.center_voxel_y);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    }
+    cudaFree(d_cs);
+    if (e != cudaSuccess) return fail(CTBB_ERR_CUDA, "rotate: %s", cudaGetErrorString(e));
+    return CTBB_OK;
+}
+
+}  // namespace
+
+using namespace ctbb;
+
+extern "C" ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* geom, const double* tube_angles_deg,
+                                              const uint64_t* slice_indices, const float* in_dev, float* out_dev,
+                                              int32_t direction) {
+    clear_error();
+    if (!ctx || !geom || !tube_angles_deg || !slice_indices || !in_dev || !out_dev)
+        return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (in_dev == out_dev) return fail(CTBB_ERR_INVALID_ARG, "in and out must not alias");
+    CTBB_CUDA(cudaSetDevice(ctx->device));
+    return rotate_device(ctx, *geom, tube_angles_deg, slice_indices, in_dev, out_dev, direction);
+}
+
+extern "C" ctbb_status ctbb_gpu_rotate(ctbb_ctx* ctx, const ctbb_geom_c* geom, const double* tube_angles_deg,
+                                       const uint64_t* slice_indices, float* vol_host, int32_t direction) {
+    clear_error();
+    if (!ctx || !geom || !tube_angles_deg || !slice_indices || !vol_host)
+        return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    CTBB_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = geom->num_voxels_x * geom->num_voxels_y * geom->num_voxels_z * sizeof(float);
+    if (bytes == 0) return CTBB_OK;
+    float *d_in = nullptr, *d_out = nullptr;
+    CTBB_CUDA(cudaMalloc(&d_in, bytes));
+    if (cudaMalloc(&d_out, bytes) != cudaSuccess) {
+        cudaFree(d_in);
+        return fail(CTBB_ERR_OOM, "rotate: device allocation failed");
+    }
+    ctbb_status rc = CTBB_OK;
+    if (cudaMemcpyAsync(d_in, vol_host, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess)
+        rc = fail(CTBB_ERR_CUDA, "rotate: upload failed");
+    if (rc == CTBB_OK) rc = rotate_device(ctx, *geom, tube_angles_deg, slice_indices, d_in, d_out, direction);
+    if (rc == CTBB_OK &&
+        (cudaMemcpyAsync(vol_host, d_out, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess ||
+         cudaStreamSynchronize(ctx->stream) != cudaSuccess))
+        rc = fail(CTBB_ERR_CUDA, "rotate: download failed");
+    cudaFree(d_in);
+    cudaFree(d_out);
+    return rc;
+}

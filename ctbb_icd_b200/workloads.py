@@ -1,0 +1,209 @@
+"""Named reconstruction workloads: parameter-file fields plus phantom spec.
+
+Each workload is the reference's parameter-file interface (the fields of
+resources/sample_prm.yaml / empty_prm.yaml) filled for one scan geometry,
+plus the seeded synthetic phantom that supplies its raw frames.
+
+Common scanner (Siemens-like, from the reference's sample_prm.yaml): source
+to isocentre 59.5 cm, source to detector 108.56 cm, channel fan increment
+0.0679 deg, quarter-detector offset 366.25 for 736 channels. Detector row
+widths are quoted at isocentre and converted to the detector
+(row_iso * SDD / R).
+
+  cfg1  plain ICD, 736 ch x 16 rows of 1.2 mm, 1152 views/turn, no FFS,
+        pitch 1, 3 turns (3456 views: 2 turns cannot hold 16 1 mm slices),
+        water phantom, I0 = 1e5, 128 x 128 x 16 at 1 mm, 25 cm FOV,
+        quadratic, lambda 1e3, 10 iterations.
+  cfg2  736 ch x 64 rows of 0.6 mm, in-plane FFS (2304 views/turn), pitch 1,
+        4 turns, water phantom + 40 random ellipsoids, I0 per view in
+        5e4..2e5, 512 x 512 x 64 at 0.6 mm, 30 cm FOV, edge-preserving with
+        delta = 5 HU (9.6e-4 cm^-1).
+  tiny, tiny_ffs, small, small_ffs, mid
+        reduced geometries (few channels/rows/views, large voxels) that the
+        reference program finishes in seconds: golden fixtures and parity
+        tests.
+"""
+from __future__ import annotations
+
+import copy
+import math
+import os
+
+MU_WATER = 0.192  # cm^-1
+SDD = 108.56
+R_SRC = 59.5
+FAN_INC_DEG = 0.0679
+
+_BASE = {
+    "FileType": 0, "FileSubType": 0, "RawOffset": 0,
+    "acquisition_fov": 50.0,
+    "focal_spot_radius": R_SRC, "source_detector_distance": SDD,
+    "anode_angle": 7.0, "axial_focal_spot_shift": 0.0375,
+    "transaxial_focal_spot_shift": 0.042698,
+    "wfbp_initialize": 0,
+}
+
+
+def _scanner(n_channels, center_channel, fan_inc_rad, n_rows, row_iso, views_wo_ffs, phi_ffs,
+             pitch, turns):
+    feed = pitch * n_rows * row_iso
+    views_per_turn = views_wo_ffs * (2 if phi_ffs else 1)
+    return {
+        "n_channels": n_channels,
+        "center_channel_non_ffs": center_channel,
+        "fan_angle_increment": fan_inc_rad,
+        "transaxial_detector_spacing": SDD * fan_inc_rad,
+        "Nrows": n_rows,
+        "center_row": (n_rows - 1) / 2.0,
+        "axial_detector_spacing": row_iso * SDD / R_SRC,
+        "CollSlicewidth": row_iso,
+        "num_views_per_turn_without_ffs": views_wo_ffs,
+        "Zffs": 0,
+        "Phiffs": 1 if phi_ffs else 0,
+        "table_feed_per_rotation": feed,
+        "Readings": turns * views_per_turn,
+    }
+
+
+def _recon(nx, fov, thickness, nz, z_start, penalty, lam, delta, iters):
+    # num_voxels_z = (size_t)(|z_end - z_start| / voxel_z) truncates
+    # (setup.cpp:237, 379): ask for nz + 0.5 slices so it lands on nz.
+    return {
+        "recon_fov": fov, "nx": nx, "ny": nx, "slice_thickness": thickness,
+        "z_start": z_start, "z_end": z_start - (nz + 0.5) * thickness,
+        "penalty": penalty, "lambda": lam, "delta": delta, "num_iterations": iters,
+    }
+
+
+FAN_INC = FAN_INC_DEG * math.pi / 180.0
+
+WORKLOADS = {
+    "cfg1": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 16, 0.12, 1152, False, 1.0, 3),
+             **_recon(128, 25.0, 0.1, 16, -1.0, "quadratic", 1e3, 0.005, 10)},
+        phantom=dict(n_ellipsoids=0, seed=0, i0_lo=1e5, i0_hi=1e5),
+    ),
+    "cfg2": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 64, 0.06, 1152, True, 1.0, 4),
+             **_recon(512, 30.0, 0.06, 64, -3.0, "edge-preserving", 0.01, 9.6e-4, 10)},
+        phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+    ),
+    # Reduced geometries (not in the benchmark): 48 channels covering the
+    # 25 cm FOV, 4 rows of 1.5 cm, 96 (or 128 x 2 with FFS) views per turn.
+    "tiny": dict(
+        prm={**_BASE,
+             **_scanner(48, 23.75, 0.00882, 4, 1.5, 96, False, 1.0, 5),
+             **_recon(16, 25.0, 1.5, 3, -5.0, "quadratic", 5.0, 0.005, 3)},
+        phantom=dict(n_ellipsoids=0, seed=1, i0_lo=1e5, i0_hi=1e5),
+    ),
+    "tiny_ffs": dict(
+        prm={**_BASE,
+             **_scanner(48, 23.75, 0.00882, 4, 1.5, 128, True, 1.0, 5),
+             **_recon(12, 25.0, 1.5, 3, -5.0, "edge-preserving", 0.5, 0.005, 3)},
+        phantom=dict(n_ellipsoids=3, seed=2, i0_lo=5e4, i0_hi=2e5, z_lo=-9.0, z_hi=-5.0),
+    ),
+    "small": dict(
+        prm={**_BASE,
+             **_scanner(96, 47.25, 0.00441, 8, 0.5, 192, False, 1.0, 4),
+             **_recon(32, 25.0, 0.5, 6, -4.0, "quadratic", 2.0, 0.005, 3)},
+        phantom=dict(n_ellipsoids=0, seed=3, i0_lo=1e5, i0_hi=1e5),
+    ),
+    "small_ffs": dict(
+        prm={**_BASE,
+             **_scanner(96, 47.25, 0.00441, 8, 0.5, 192, True, 1.0, 4),
+             **_recon(32, 25.0, 0.5, 6, -4.0, "edge-preserving", 0.2, 0.005, 3)},
+        phantom=dict(n_ellipsoids=6, seed=4, i0_lo=5e4, i0_hi=2e5, z_lo=-7.0, z_hi=-4.0),
+    ),
+    "mid": dict(
+        prm={**_BASE,
+             **_scanner(368, 183.25, 0.00118508 * 2, 16, 0.24, 576, False, 1.0, 3),
+             **_recon(64, 25.0, 0.2, 8, -1.5, "quadratic", 50.0, 0.005, 3)},
+        phantom=dict(n_ellipsoids=0, seed=5, i0_lo=1e5, i0_hi=1e5),
+    ),
+}
+
+PRM_ORDER = [
+    "sinogram_path", "output_dir", "output_file", "initial_recon_path", "matrix_path",
+    "FileType", "FileSubType", "RawOffset", "Readings",
+    "acquisition_fov", "n_channels", "num_views_per_turn_without_ffs", "focal_spot_radius",
+    "source_detector_distance", "anode_angle", "axial_detector_spacing",
+    "axial_focal_spot_shift", "center_channel_non_ffs", "center_row",
+    "transaxial_detector_spacing", "transaxial_focal_spot_shift", "fan_angle_increment",
+    "table_feed_per_rotation", "Zffs", "Phiffs", "Nrows", "CollSlicewidth",
+    "recon_fov", "nx", "ny", "slice_thickness", "z_start", "z_end",
+    "wfbp_initialize", "penalty", "lambda", "delta", "num_iterations",
+]
+
+
+def workload(name: str) -> dict:
+    return copy.deepcopy(WORKLOADS[name])
+
+
+def prm_text(prm: dict) -> str:
+    """Parameter file text in the reference's flat YAML form."""
+    lines = ["# generated by ctbb_icd_b200.workloads"]
+    keys = [k for k in PRM_ORDER if k in prm] + [k for k in prm if k not in PRM_ORDER]
+    for k in keys:
+        v = prm[k]
+        if isinstance(v, float):
+            v = repr(v)
+        lines.append(f"{k}: {v}")
+    return "\n".join(lines) + "\n"
+
+
+def write_prm(path: str, prm: dict) -> str:
+    with open(path, "w") as f:
+        f.write(prm_text(prm))
+    return path
+
+
+def phantom_spec(name_or_dict):
+    """ctypes PhantomSpec for a workload (or a workload's phantom dict)."""
+    from ._lib import PhantomSpec
+
+    ph = name_or_dict if isinstance(name_or_dict, dict) else WORKLOADS[name_or_dict]["phantom"]
+    prm = None if isinstance(name_or_dict, dict) else WORKLOADS[name_or_dict]["prm"]
+    spec = PhantomSpec()
+    spec.n_ellipsoids = int(ph.get("n_ellipsoids", 0))
+    spec.seed = int(ph.get("seed", 0))
+    if "z_lo" in ph:
+        spec.ellipsoid_z_lo, spec.ellipsoid_z_hi = float(ph["z_lo"]), float(ph["z_hi"])
+    elif prm is not None:
+        spec.ellipsoid_z_lo = float(min(prm["z_start"], prm["z_end"]))
+        spec.ellipsoid_z_hi = float(max(prm["z_start"], prm["z_end"]))
+    spec.i0_lo = float(ph.get("i0_lo", 0.0))
+    spec.i0_hi = float(ph.get("i0_hi", 0.0))
+    return spec
+
+
+def materialise(name: str, directory: str, *, raw: bool = True, n_threads: int | None = None,
+                overrides: dict | None = None):
+    """Write <directory>/<name>.prm (and the synthetic raw file) for a workload.
+
+    Returns (prm_path, ReconParams). The raw file is produced by the CPU
+    projector (ctbb_synth_raw_host) in FileType 0 layout.
+    """
+    from . import configure_recon_params, synth_raw_host, write_raw_file
+
+    w = workload(name)
+    prm = w["prm"]
+    if overrides:
+        prm.update(overrides)
+    os.makedirs(os.path.join(directory, "reconstructions"), exist_ok=True)
+    prm.setdefault("sinogram_path", os.path.join(directory, f"{name}.bin"))
+    prm.setdefault("output_dir", directory)
+    prm.setdefault("output_file", f"{name}.img")
+    prm_path = write_prm(os.path.join(directory, f"{name}.prm"), prm)
+    if raw and not os.path.exists(prm["sinogram_path"]):
+        open(prm["sinogram_path"], "wb").close()  # load_raw wants the file to exist
+    rp = configure_recon_params(prm_path)
+    if raw:
+        spec_dict = dict(w["phantom"])
+        if "z_lo" not in spec_dict:
+            spec_dict["z_lo"] = min(prm["z_start"], prm["z_end"])
+            spec_dict["z_hi"] = max(prm["z_start"], prm["z_end"])
+        data = synth_raw_host(rp, spec_dict, n_threads=n_threads or os.cpu_count() or 1)
+        write_raw_file(prm["sinogram_path"], rp, data)
+    return prm_path, rp

@@ -1,0 +1,342 @@
+/*
+ * ctbb_icd_b200 — C ABI of the B200 reconstruction path for CTBB_ICD.
+ *
+ * The reference program (CTBB_ICD) runs one host-thread pipeline of C++ free
+ * functions  void stage(const recon_params*, ct_data*)  in this order
+ * (src/main.cpp:88-128):
+ *
+ *   configure_recon_params -> load_raw -> initialize_recon_volume
+ *     -> generate_system_matrix[_ffs] -> icd_iteration
+ *     -> rotate_slices_rotating2fixed -> clean_up
+ *
+ * This header is the drop-in boundary for the numerical stages of that flow.
+ * Every entry point is extern "C", takes plain pointers and sizes, returns a
+ * ctbb_status (never exits), and names the reference function it replaces.
+ * recon_params is not POD (std::string members, src/recon_structs.h:27-33),
+ * so its numeric fields cross the boundary as ctbb_geom_c, in the same order,
+ * with the same names and units (cm, radians; tube angles in degrees).
+ *
+ * Threading: one host thread per context. Device memory is owned by the
+ * context / ssm / recon objects; host buffers are only borrowed for the call.
+ */
+#ifndef CTBB_ICD_B200_H
+#define CTBB_ICD_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------------- */
+/* Status codes                                                              */
+/* ------------------------------------------------------------------------- */
+typedef int32_t ctbb_status;
+enum {
+    CTBB_OK = 0,
+    CTBB_ERR_INVALID_ARG = 1, /* null pointer, bad size, inconsistent geometry   */
+    CTBB_ERR_CONFIG = 2,      /* missing/invalid parameter-file field            */
+    CTBB_ERR_IO = 3,          /* file missing, short read, write failure         */
+    CTBB_ERR_RANGE = 4,       /* requested z-range outside the scanned data      */
+    CTBB_ERR_CUDA = 5,        /* CUDA runtime error (message in ctbb_last_error) */
+    CTBB_ERR_NO_DEVICE = 6,   /* no CUDA device / library built without CUDA     */
+    CTBB_ERR_OOM = 7,         /* device or host allocation failed                */
+    CTBB_ERR_TIMEOUT = 8,     /* a bounded device wait gave up                   */
+    CTBB_ERR_UNSUPPORTED = 9, /* feature not available (e.g. PTR/IMA readers)    */
+    CTBB_ERR_FORMAT = 10      /* corrupt or mismatched matrix file               */
+};
+
+/* Penalty selector (recon_params.penalty string, src/setup.cpp:169-174). */
+enum { CTBB_PENALTY_QUADRATIC = 0, CTBB_PENALTY_EDGE_PRESERVING = 1 };
+
+/*
+ * Numeric fields of recon_params (src/recon_structs.h:25-114), same order,
+ * names and units. size_t fields are uint64_t; the `penalty` string becomes
+ * an enum at the position the string occupied.
+ */
+typedef struct ctbb_geom_c {
+    /* Scanner geometry */
+    double acquisition_fov;
+    double anode_angle;
+    double axial_detector_spacing;
+    double axial_focal_spot_shift;
+    double center_channel_non_ffs;
+    double center_row;
+    double focal_spot_radius;
+    uint64_t n_channels;
+    uint64_t num_views_per_turn;
+    uint64_t num_views_per_turn_without_ffs;
+    double source_detector_distance;
+    double transaxial_detector_spacing;
+    double transaxial_focal_spot_shift;
+    double fan_angle_increment;
+    /* Iterative recon parameters */
+    int32_t penalty; /* CTBB_PENALTY_* */
+    int32_t reserved0;
+    double lambda;
+    double delta;
+    uint64_t num_iterations;
+    /* Scan specific parameters */
+    uint64_t Nrows;
+    double first_view_angle;
+    uint64_t num_z_ffs;
+    uint64_t num_phi_ffs;
+    uint64_t num_views;
+    double table_feed_per_rotation;
+    double tube_angle_increment;
+    double z_end;
+    double z_first_view;
+    double z_good_slice;
+    double z_matrix_start;
+    double z_start;
+    int32_t table_direction;
+    int32_t reserved1;
+    /* Recon geometry */
+    double fov_radius;
+    double center_voxel_x;
+    double center_voxel_y;
+    double center_voxel_z;
+    double dx;
+    double dy;
+    double dz;
+    uint64_t nx;
+    uint64_t ny;
+    uint64_t nz;
+    /* Raw-file and scan mode fields */
+    uint64_t FileType;
+    uint64_t FileSubType;
+    uint64_t RawOffset;
+    uint64_t Readings;
+    uint64_t Zffs;
+    uint64_t Phiffs;
+    double CollSlicewidth;
+    uint64_t wfbp_initialize;
+    /* Derived values */
+    uint64_t Nrows_projection;
+    uint64_t views_per_slice;
+    double voxel_size_x;
+    double voxel_size_y;
+    double voxel_size_z;
+    double tube_z_increment;
+    double beam_width;
+    double beam_width_at_roi_edge;
+    uint64_t num_views_for_system_matrix;
+    uint64_t num_voxels_x;
+    uint64_t num_voxels_y;
+    uint64_t num_voxels_z;
+    double slice_thickness;
+    double recon_fov;
+} ctbb_geom_c;
+
+/* ------------------------------------------------------------------------- */
+/* Host-side setup (no GPU needed)                                           */
+/* ------------------------------------------------------------------------- */
+
+/* Last error message of the calling thread (empty string if none). */
+const char* ctbb_last_error(void);
+const char* ctbb_status_str(ctbb_status s);
+
+/*
+ * Parse a parameter file, apply the reference's required-field checks and
+ * defaults, and compute the derived values.
+ * Replaces configure_recon_params (src/setup.cpp:69-243) and parse_config
+ * (src/parse_config.cpp:34-111). String fields are returned through the
+ * optional buffers (NULL to skip, each `cap` bytes).
+ */
+typedef struct ctbb_prm_strings {
+    char initial_recon_path[1024];
+    char matrix_path[1024];
+    char output_dir[1024];
+    char output_file[1024];
+    char potential[64];
+    char recon_path[1024];
+    char sinogram_path[1024];
+    char penalty[64];
+} ctbb_prm_strings;
+
+ctbb_status ctbb_configure_recon_params(const char* prm_path, ctbb_geom_c* geom,
+                                        ctbb_prm_strings* strings);
+
+/*
+ * Tube angles, table positions and the rotating-slice tables, plus the final
+ * table_direction / z_first_view / num_voxels_z, for FileType 0 data.
+ * Replaces the geometry part of load_raw (src/setup.cpp:273-285, 348-409).
+ * tube_angles / table_positions hold Readings values; slice_locations /
+ * slice_indices hold up to max_slices values (the count is geom->num_voxels_z
+ * on return). Returns CTBB_ERR_RANGE for the reference's invalid-range exit.
+ */
+ctbb_status ctbb_slice_tables(ctbb_geom_c* geom, double* tube_angles, double* table_positions,
+                              double* slice_locations, uint64_t* slice_indices,
+                              uint64_t max_slices);
+
+/*
+ * Read FileType 0 frames into raw[Readings][n_channels][Nrows_projection]
+ * (row fastest). Replaces the ReadBinaryFrame loop and the two transposes of
+ * load_raw (src/setup.cpp:271-299, 334-344).
+ */
+ctbb_status ctbb_read_raw(const char* path, const ctbb_geom_c* geom, float* raw);
+
+/* ------------------------------------------------------------------------- */
+/* Synthetic data (stands in for the private ctbb_read library)              */
+/* ------------------------------------------------------------------------- */
+typedef struct ctbb_phantom_spec {
+    int32_t n_ellipsoids;  /* random ellipsoids added to the water phantom   */
+    int32_t reserved;
+    uint64_t seed;         /* phantom and noise seed                        */
+    double ellipsoid_z_lo; /* z range (cm, fixed frame) of ellipsoid centres */
+    double ellipsoid_z_hi;
+    double i0_lo;          /* incident photons per ray; <= 0 -> noise free  */
+    double i0_hi;          /* > i0_lo -> drawn per view in [i0_lo, i0_hi]   */
+} ctbb_phantom_spec;
+
+/* CPU projector: writes raw[Readings][n_channels][Nrows_projection]. */
+ctbb_status ctbb_synth_raw_host(const ctbb_geom_c* geom, const ctbb_phantom_spec* spec,
+                                float* raw, int n_threads);
+/* Write raw as a FileType 0 file (frames channel-major, row fastest). */
+ctbb_status ctbb_write_raw_file(const char* path, const ctbb_geom_c* geom, const float* raw);
+
+/* ------------------------------------------------------------------------- */
+/* GPU context                                                               */
+/* ------------------------------------------------------------------------- */
+typedef struct ctbb_ctx ctbb_ctx;
+typedef struct ctbb_ssm ctbb_ssm;
+typedef struct ctbb_recon ctbb_recon;
+
+/* stream: a cudaStream_t to run on, or NULL for a context-owned stream. */
+ctbb_status ctbb_gpu_init(int device, void* stream, ctbb_ctx** out);
+void ctbb_gpu_destroy(ctbb_ctx* ctx);
+/* The cudaStream_t all work of this context is issued on. */
+void* ctbb_gpu_stream(ctbb_ctx* ctx);
+ctbb_status ctbb_gpu_synchronize(ctbb_ctx* ctx);
+
+/* GPU projector writing a device buffer raw_dev of Readings*n_ch*n_rows floats. */
+ctbb_status ctbb_gpu_synth_raw(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                               const ctbb_phantom_spec* spec, float* raw_dev);
+
+/* ------------------------------------------------------------------------- */
+/* Stored system matrix                                                      */
+/* ------------------------------------------------------------------------- */
+enum { CTBB_SSM_FP32 = 1, CTBB_SSM_FP16 = 2, CTBB_SSM_BOTH = 3 };
+
+typedef struct ctbb_ssm_info {
+    uint64_t n_columns;     /* num_voxels_x * num_voxels_y                 */
+    uint64_t n_views;       /* num_views_for_system_matrix                 */
+    uint64_t nnz;           /* stored entries                              */
+    uint64_t max_col_nnz;   /* largest column                              */
+    uint64_t bytes_device;  /* device bytes held by the matrix             */
+    int32_t weights;        /* CTBB_SSM_* held                             */
+    int32_t ffs;            /* 1 if built with the in-plane flying focal spot */
+    double build_ms;        /* device time of the last build               */
+} ctbb_ssm_info;
+
+/*
+ * Build the stored system matrix on the device: per voxel column (i + nx*j),
+ * entries (q, w) with q = row + Nrows*(channel + n_channels*view), sorted by q.
+ * Chooses the in-plane FFS model when geom->Phiffs is set.
+ * Replaces generate_system_matrix (src/generate_system_matrix.cpp:54-209) and
+ * generate_system_matrix_ffs (src/generate_system_matrix_ffs.cpp:60-239);
+ * the on-disk matrix.bin round trip (:212-303) becomes an HBM-resident matrix.
+ */
+ctbb_status ctbb_gpu_generate_ssm(ctbb_ctx* ctx, const ctbb_geom_c* geom, int32_t weights,
+                                  ctbb_ssm** out);
+ctbb_status ctbb_gpu_ssm_info(const ctbb_ssm* ssm, ctbb_ssm_info* info);
+/* Copy one column to host: nnz returned; idx/w may be NULL to query size. */
+ctbb_status ctbb_gpu_ssm_column(const ctbb_ssm* ssm, uint64_t column, int32_t* idx, float* w,
+                                uint64_t cap, uint64_t* nnz);
+/*
+ * Write / read the reference's matrix.bin layout: per column, a size_t count
+ * then count x {int32 index, float32 value} (src/generate_system_matrix.cpp:212-303,
+ * read back at src/icd_iteration.cpp:164-179).
+ */
+ctbb_status ctbb_gpu_ssm_export_reference(const ctbb_ssm* ssm, const char* path);
+ctbb_status ctbb_gpu_ssm_import_reference(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                                          const char* path, int32_t weights, ctbb_ssm** out);
+void ctbb_gpu_ssm_free(ctbb_ssm* ssm);
+
+/* ------------------------------------------------------------------------- */
+/* ICD reconstruction                                                        */
+/* ------------------------------------------------------------------------- */
+enum {
+    CTBB_ICD_SEQUENTIAL = 0, /* reference visiting order, FP64 state (parity mode) */
+    CTBB_ICD_GROUPED = 1     /* many voxels in flight, FP32 error sinogram         */
+};
+
+typedef struct ctbb_icd_opts {
+    int32_t mode;             /* CTBB_ICD_*                                       */
+    int32_t weights;          /* grouped mode: CTBB_SSM_FP32 or CTBB_SSM_FP16     */
+    int32_t refresh_every;    /* grouped: FP64 y - Ax refresh every K iterations (0: never) */
+    int32_t warps_in_flight;  /* grouped: concurrent voxel updates (0: autotune)  */
+    int32_t lattice;          /* grouped: in-plane spacing of the visiting order (0: auto) */
+    int32_t compute_cost;     /* evaluate the FP64 cost after each iteration      */
+    double stop_rel_change;   /* stop when |dcost|/cost < this (0: fixed count)   */
+} ctbb_icd_opts;
+
+typedef struct ctbb_iter_stats {
+    int32_t iterations;       /* iterations run by the call                       */
+    int32_t reserved;
+    double cost;              /* FP64 cost after the last iteration (if computed) */
+    double rel_change;        /* |dcost|/cost of the last iteration               */
+    double device_ms;         /* device time of the ICD kernels in the call       */
+    double voxel_updates;     /* voxel updates performed                          */
+    double entries;           /* SSM entries visited (sum of in-range nnz)        */
+} ctbb_iter_stats;
+
+/*
+ * Device-resident reconstruction state for one volume: raw data y, the
+ * current iterate x ([nz][ny][nx], rotating frame) and the error sinogram
+ * e = y - Ax. slice_indices holds nz central view indices (load_raw).
+ */
+ctbb_status ctbb_gpu_recon_create(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                                  const uint64_t* slice_indices, ctbb_recon** out);
+void ctbb_gpu_recon_free(ctbb_recon* rc);
+ctbb_status ctbb_gpu_recon_set_raw(ctbb_recon* rc, const float* raw_host);
+ctbb_status ctbb_gpu_recon_set_raw_device(ctbb_recon* rc, const float* raw_dev);
+/* Device pointer of the recon's raw buffer (for the GPU projector). */
+float* ctbb_gpu_recon_raw_device(ctbb_recon* rc);
+/* Initial image (host, float [nz][ny][nx]); NULL -> zeros. Resets e = y - Ax. */
+ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host);
+ctbb_status ctbb_gpu_recon_get_volume(ctbb_recon* rc, float* vol_host);
+ctbb_status ctbb_gpu_recon_get_volume_f64(ctbb_recon* rc, double* vol_host);
+/* Run n_iter ICD iterations. */
+ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts* opts,
+                                   int32_t n_iter, ctbb_iter_stats* stats);
+/* Recompute e = y - Ax with FP64 accumulation. */
+ctbb_status ctbb_gpu_recon_refresh_residual(ctbb_recon* rc, const ctbb_ssm* ssm);
+/* FP64 cost of the current iterate (quadratic: 1/2|e|^2 + lambda/4 sum w dx^2;
+ * edge-preserving: |e|^2 + lambda/2 sum w rho(dx)). */
+ctbb_status ctbb_gpu_recon_cost(ctbb_recon* rc, double* cost);
+
+/*
+ * One-call drop-in for icd_iteration (src/icd_iteration.cpp:42-286): copies
+ * raw and recon_volume (initial image) from the host, runs
+ * geom->num_iterations iterations and writes the result back to recon_volume.
+ */
+ctbb_status ctbb_gpu_icd(ctbb_ctx* ctx, const ctbb_ssm* ssm, const ctbb_geom_c* geom,
+                         const uint64_t* slice_indices, const float* raw, float* recon_volume,
+                         const ctbb_icd_opts* opts, ctbb_iter_stats* stats);
+
+/* ------------------------------------------------------------------------- */
+/* Slice rotation                                                            */
+/* ------------------------------------------------------------------------- */
+enum { CTBB_ROTATE_FIXED2ROTATING = 1, CTBB_ROTATE_ROTATING2FIXED = -1 };
+
+/*
+ * Rotate every slice k by the tube angle of its central view with bilinear
+ * interpolation and a zero border, host volume in place.
+ * Replaces rotate_slices_rotating2fixed (src/rotate_slices.cpp:81-114),
+ * rotate_slices_fixed2rotating (:48-79), rotate_slice (:116-154) and
+ * interp2 (src/interp.h:41-76).
+ */
+ctbb_status ctbb_gpu_rotate(ctbb_ctx* ctx, const ctbb_geom_c* geom, const double* tube_angles_deg,
+                            const uint64_t* slice_indices, float* vol_host, int32_t direction);
+/* Same on device buffers (in and out must not alias). */
+ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                                   const double* tube_angles_deg, const uint64_t* slice_indices,
+                                   const float* in_dev, float* out_dev, int32_t direction);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CTBB_ICD_B200_H */
