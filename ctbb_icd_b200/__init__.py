@@ -251,11 +251,12 @@ class Ssm:
 
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
-             compute_cost=False, stop_rel_change=0.0) -> IcdOpts:
+             compute_cost=False, stop_rel_change=0.0, relax=0.0) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
     o.compute_cost, o.stop_rel_change = int(bool(compute_cost)), float(stop_rel_change)
+    o.relax = float(relax)
     return o
 
 
@@ -277,6 +278,11 @@ class Recon:
 
     def set_raw_device(self, dev_ptr: int):
         check(lib().ctbb_gpu_recon_set_raw_device(self.handle, C.c_void_p(dev_ptr)))
+
+    def raw(self) -> np.ndarray:
+        out = np.empty(self.rp.raw_shape, np.float32)
+        check(lib().ctbb_gpu_recon_get_raw(self.handle, ptr(out, C.c_float)))
+        return out
 
     def raw_device_ptr(self) -> int:
         return lib().ctbb_gpu_recon_raw_device(self.handle) or 0
@@ -300,6 +306,12 @@ class Recon:
         o = opts or icd_opts()
         check(lib().ctbb_gpu_recon_iterate(self.handle, ssm.handle, C.byref(o), int(n_iter), C.byref(st)))
         return st
+
+    def entries(self, ssm: Ssm) -> float:
+        """In-range matrix entries one iteration visits (sum over voxels)."""
+        e = C.c_double()
+        check(lib().ctbb_gpu_recon_entries(self.handle, ssm.handle, C.byref(e)))
+        return e.value
 
     def refresh_residual(self, ssm: Ssm):
         check(lib().ctbb_gpu_recon_refresh_residual(self.handle, ssm.handle))

@@ -98,7 +98,7 @@ class SsmInfo(C.Structure):
 class IcdOpts(C.Structure):
     _fields_ = [
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
-        ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D),
+        ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
     ]
 
 
@@ -141,10 +141,12 @@ PROTOTYPES = {
     "ctbb_gpu_recon_set_raw": (_I, [_P, _PF]),
     "ctbb_gpu_recon_set_raw_device": (_I, [_P, _P]),
     "ctbb_gpu_recon_raw_device": (_P, [_P]),
+    "ctbb_gpu_recon_get_raw": (_I, [_P, _PF]),
     "ctbb_gpu_recon_set_volume": (_I, [_P, _P, _PF]),
     "ctbb_gpu_recon_get_volume": (_I, [_P, _PF]),
     "ctbb_gpu_recon_get_volume_f64": (_I, [_P, _PD]),
     "ctbb_gpu_recon_iterate": (_I, [_P, _P, C.POINTER(IcdOpts), _I, C.POINTER(IterStats)]),
+    "ctbb_gpu_recon_entries": (_I, [_P, _P, _PD]),
     "ctbb_gpu_recon_refresh_residual": (_I, [_P, _P]),
     "ctbb_gpu_recon_cost": (_I, [_P, _PD]),
     "ctbb_gpu_icd": (_I, [_P, _P, _PG, _PU, _PF, _PF, C.POINTER(IcdOpts), C.POINTER(IterStats)]),

@@ -73,6 +73,9 @@ struct ctbb_recon {
     float* d_x32 = nullptr;      // grouped-mode image
     float* d_e32 = nullptr;      // grouped-mode y - A x
     int rep = 0;                 // 0: x64/est64 current, 1: x32/e32 current
+    // Sum over voxels inside the FOV of in-range matrix entries (cached per matrix).
+    const ctbb_ssm* entries_ssm = nullptr;
+    double entries = 0.0;
 };
 
 namespace ctbb {
@@ -95,5 +98,6 @@ ctbb_status launch_icd_sequential(ctbb_recon* rc, const ctbb_ssm* ssm, int n_ite
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o,
                                float* ms, double* entries);
 int default_warps_in_flight(const ctbb_recon* rc);
+ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out);
 
 }  // namespace ctbb

@@ -40,9 +40,10 @@ namespace {
 
 struct GParams {
     int nx, ny, nz, nch, nr, nvsm, readings, penalty;
-    int P, Q, mx, my, kq, n_offsets, stride;
+    int P, Q, mx, my, kq, n_offsets, stride, pstride;
     uint64_t n_items, per_offset, per_residue, nvsm1;
     float lambda, delta;
+    double relax;  // step scale applied to the exact 1-D update before the positivity clamp
     double cvx, cvy, vx, vy, fov_limit;
 };
 
@@ -105,8 +106,11 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64
         const int pt = (int)(rem / P.kq);
         const int kk = (int)(rem % P.kq);
         const int os = (int)(((uint64_t)o * P.stride) % P.n_offsets);
-        const int i = os % P.P + P.P * (pt % P.mx);
-        const int j = os / P.P + P.P * (pt / P.mx);
+        // Golden-ratio stride over the lattice points spreads consecutive
+        // items (and hence the items in flight) over the whole slice.
+        const int ps = (int)(((uint64_t)pt * P.pstride) % (uint64_t)(P.mx * P.my));
+        const int i = os % P.P + P.P * (ps % P.mx);
+        const int j = os / P.P + P.P * (ps / P.mx);
         const int k = r + P.Q * kk;
         if (i >= P.nx || j >= P.ny || k >= P.nz) continue;
         const double xx = (i - P.cvx) * P.vx, yy = (j - P.cvy) * P.vy;
@@ -201,6 +205,7 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64
             }
             upd = c;
         }
+        upd *= P.relax;
         if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
         if (lane == 0) x[q] = (float)(xq + upd);
         const float du = (float)upd;
@@ -211,22 +216,32 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64
     }
 }
 
-}  // namespace
-
-namespace ctbb {
-
-int default_warps_in_flight(const ctbb_recon* rc) {
-    // Keep (voxels crossed per ray) * W / N near 0.4; a ray crosses about
-    // 4 * 0.8 * nx voxels (2 in-plane bilinear taps x 2 slices per x step).
-    const double n = (double)rc->nvox;
-    const double per_ray = 3.2 * (double)rc->geom.num_voxels_x;
-    int w = (int)(0.4 * n / per_ray);
-    const int lo = 64, hi = rc->ctx->sm_count * 32;
-    return std::max(lo, std::min(hi, w));
+// Sum of in-range entries over (column inside the FOV, slice): the unit of
+// work of one iteration. One warp per column.
+__global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uint32_t* __restrict__ vptr,
+                                                            const int32_t* __restrict__ start,
+                                                            unsigned long long* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t col = warp; col < ncol; col += nwarps) {
+        const int i = (int)(col % P.nx), j = (int)(col / P.nx);
+        const double xx = (i - P.cvx) * P.vx, yy = (j - P.cvy) * P.vy;
+        if (!(xx * xx + yy * yy < P.fov_limit)) continue;
+        unsigned long long s = 0;
+        for (int k = lane; k < P.nz; k += 32) {
+            const int st = start[k];
+            const int v0 = max(0, -st), v1 = min(P.nvsm, P.readings - st);
+            if (v1 > v0) s += vptr[col * P.nvsm1 + v1] - vptr[col * P.nvsm1 + v0];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) atomicAdd(out, s);
+    }
 }
 
-ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
-                               double* entries) {
+GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o) {
     const ctbb_geom_c& g = rc->geom;
     GParams P;
     P.nx = (int)g.num_voxels_x;
@@ -257,17 +272,63 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     };
     while (gcd(stride, P.n_offsets) != 1) ++stride;
     P.stride = stride;
+    const int npts = P.mx * P.my;
+    int ps = std::max(1, (int)(0.6180339887 * npts));
+    while (npts > 1 && gcd(ps, npts) != 1) ++ps;
+    P.pstride = ps;
     P.per_residue = (uint64_t)P.mx * P.my * P.kq;
     P.per_offset = P.per_residue * P.Q;
     P.n_items = P.per_offset * P.n_offsets;
     P.lambda = (float)g.lambda;
     P.delta = (float)g.delta;
+    P.relax = (o.relax > 0.0 && o.relax < 2.0) ? o.relax : 1.0;
     P.cvx = g.center_voxel_x;
     P.cvy = g.center_voxel_y;
     P.vx = g.voxel_size_x;
     P.vy = g.voxel_size_y;
     P.fov_limit = (g.acquisition_fov / 2.0) * (g.acquisition_fov / 2.0);
 
+    return P;
+}
+
+
+}  // namespace
+
+namespace ctbb {
+
+ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out) {
+    if (rc->entries_ssm != ssm) {
+        ctbb_icd_opts o{};
+        const GParams P = make_params(rc, ssm, o);
+        ctbb_ctx* ctx = rc->ctx;
+        unsigned long long* d = ctx->d_queue + 1;
+        CTBB_CUDA(cudaMemsetAsync(d, 0, sizeof(unsigned long long), ctx->stream));
+        count_entries_kernel<<<ctx->sm_count * 8, 256, 0, ctx->stream>>>(P, ssm->d_vptr, rc->d_start, d);
+        CTBB_CUDA(cudaGetLastError());
+        unsigned long long h = 0;
+        CTBB_CUDA(cudaMemcpyAsync(&h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+        CTBB_CUDA(cudaStreamSynchronize(ctx->stream));
+        rc->entries = (double)h;
+        rc->entries_ssm = ssm;
+    }
+    *out = rc->entries;
+    return CTBB_OK;
+}
+
+int default_warps_in_flight(const ctbb_recon* rc) {
+    // Keep (voxels crossed per ray) * W / N near 0.4; a ray crosses about
+    // 4 * 0.8 * nx voxels (2 in-plane bilinear taps x 2 slices per x step).
+    const double n = (double)rc->nvox;
+    const double per_ray = 3.2 * (double)rc->geom.num_voxels_x;
+    int w = (int)(0.4 * n / per_ray);
+    const int lo = 4, hi = rc->ctx->sm_count * 32;
+    return std::max(lo, std::min(hi, w));
+}
+
+ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
+                               double* entries) {
+    const GParams P = make_params(rc, ssm, o);
+    if (entries) CTBB_TRY(inrange_entries(rc, ssm, entries));
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
     const int blocks = std::max(1, (W + 7) / 8);
     ctbb_ctx* ctx = rc->ctx;
@@ -290,7 +351,6 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     cudaEventElapsedTime(ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (entries) *entries = 0.0;
     return CTBB_OK;
 }
 

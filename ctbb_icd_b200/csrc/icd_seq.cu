@@ -9,9 +9,8 @@
 //
 // One 1024-thread block walks the voxels in order (each update depends on
 // the previous one). The block splits a column's entries across threads,
-// reduces alpha/beta in FP64, one thread evaluates the penalty exactly as
-// the reference does (bisection included), and the block scatters the
-// update. Only the summation order of alpha/beta differs from the
+// reduces alpha/beta in FP64, one warp evaluates the penalty exactly as the
+// reference does (bisection included), and the block scatters the update. Only the summation order of alpha/beta differs from the
 // reference's OpenMP reduction. Compiled with -fmad=false.
 #include "gpu_internal.h"
 
@@ -53,48 +52,57 @@ __device__ double quadratic_update(int q, double alpha, double beta, double lamb
     return (beta + lambda * sum) / (alpha + lambda * ws);
 }
 
-// penalties.cpp:141-154
-__device__ double edge_f(double du, double alpha, double beta, double delta, double lambda, const double* xn, int valid,
-                         double xq) {
-    double sum = 0.0;
-    for (int i = 0; i < 8; ++i) {
-        if (valid & (1 << i)) {
-            const double t = du - (xn[i] - xq);
-            if (t >= 0)
-                sum = sum + W8(i) * (1.0 - 1.0 / (1.0 + fabs(t / delta)));
-            else
-                sum = sum - W8(i) * (1.0 - 1.0 / (1.0 + fabs(t / delta)));
-        }
-    }
-    return 2 * alpha * du - 2 * beta + lambda * sum;
-}
-
-// penalties.cpp:88-139 (bisection; f(a) is a pure function of a, so it is
-// cached instead of being re-evaluated each step).
-__device__ double edge_update(int q, double alpha, double beta, double lambda, double delta, size_t nx, size_t nvox,
-                              const double* x) {
+// penalties.cpp:88-154 (bisection on func) evaluated by one warp: lanes 0-7
+// compute the eight neighbour terms of func in parallel and every lane then
+// adds them in the order i = 0..7, so each f(d) (and hence the bisection
+// path) is bit-identical to the serial evaluation. f(a) is a pure function of
+// a, so it is carried along instead of being re-evaluated each step.
+__device__ double edge_update_warp(int q, double alpha, double beta, double lambda, double delta, size_t nx,
+                                   size_t nvox, const double* x) {
+    const int lane = threadIdx.x & 31;
     size_t nb[8];
     neighbours(q, nx, nb);
     if (alpha == 0.0) return 0.0;
     const double xq = x[q];
-    double xn[8];
-    int valid = 0;
+    double xn = 0.0, wl = 0.0;
+    bool valid = false;
+    if (lane < 8) {
+        size_t n = nb[0];
+#pragma unroll
+        for (int i = 1; i < 8; ++i)
+            if (lane == i) n = nb[i];
+        valid = n < nvox;
+        if (valid) xn = x[n];
+        wl = W8(lane);
+    }
+    const unsigned vmask = __ballot_sync(0xffffffffu, valid);
     double a = beta / alpha, b = beta / alpha;
     for (int i = 0; i < 8; ++i) {
-        xn[i] = 0.0;
-        if (nb[i] < nvox) {
-            valid |= 1 << i;
-            xn[i] = x[nb[i]];
-            const double d = xn[i] - xq;
+        const double d = __shfl_sync(0xffffffffu, xn, i) - xq;
+        if (vmask & (1u << i)) {
             if (d < a) a = d;
             if (d > b) b = d;
         }
     }
-    double fa = edge_f(a, alpha, beta, delta, lambda, xn, valid, xq);
+    auto f = [&](double du) {
+        double term = 0.0;
+        if (valid) {
+            const double t = du - (xn - xq);
+            const double g = 1.0 - 1.0 / (1.0 + fabs(t / delta));
+            term = (t >= 0) ? wl * g : -(wl * g);
+        }
+        double sum = 0.0;
+        for (int i = 0; i < 8; ++i) {
+            const double v = __shfl_sync(0xffffffffu, term, i);
+            if (vmask & (1u << i)) sum = sum + v;
+        }
+        return 2 * alpha * du - 2 * beta + lambda * sum;
+    };
+    double fa = f(a);
     double c = (a + b) / 2.0;
     for (int it = 0; it < 1000000; ++it) {
         c = (a + b) / 2.0;
-        const double fc = edge_f(c, alpha, beta, delta, lambda, xn, valid, xq);
+        const double fc = f(c);
         if (fc == 0 || (b - a) / 2 < 0.00000001) return c;
         const int sc = fc < 0 ? -1 : 1, sa = fa < 0 ? -1 : 1;
         if (sc == sa) {
@@ -155,18 +163,23 @@ __global__ void __launch_bounds__(1024) icd_seq_kernel(SeqParams P, const int64_
                     sb[wid] = beta;
                 }
                 __syncthreads();
-                if (tid == 0) {
+                if (wid == 0) {
                     double A = 0.0, B = 0.0;
                     for (int t = 0; t < nw; ++t) {
                         A += sa[t];
                         B += sb[t];
                     }
-                    double upd = (P.penalty == CTBB_PENALTY_QUADRATIC)
-                                     ? quadratic_update(q, A, B, P.lambda, nxs, nvox, x)
-                                     : edge_update(q, A, B, P.lambda, P.delta, nxs, nvox, x);
-                    if (upd + x[q] < 0) upd = -x[q];
-                    x[q] += upd;
-                    s_upd = upd;
+                    double upd;
+                    if (P.penalty == CTBB_PENALTY_QUADRATIC) {
+                        upd = quadratic_update(q, A, B, P.lambda, nxs, nvox, x);
+                    } else {
+                        upd = edge_update_warp(q, A, B, P.lambda, P.delta, nxs, nvox, x);
+                    }
+                    if (lane == 0) {
+                        if (upd + x[q] < 0) upd = -x[q];
+                        x[q] += upd;
+                        s_upd = upd;
+                    }
                 }
                 __syncthreads();
                 const double upd = s_upd;

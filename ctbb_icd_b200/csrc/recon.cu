@@ -317,6 +317,16 @@ extern "C" ctbb_status ctbb_gpu_recon_set_raw_device(ctbb_recon* rc, const float
 
 extern "C" float* ctbb_gpu_recon_raw_device(ctbb_recon* rc) { return rc ? rc->d_raw : nullptr; }
 
+extern "C" ctbb_status ctbb_gpu_recon_get_raw(ctbb_recon* rc, float* raw_host) {
+    clear_error();
+    if (!rc || !raw_host) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    CTBB_CUDA(cudaSetDevice(rc->ctx->device));
+    CTBB_CUDA(cudaMemcpyAsync(raw_host, rc->d_raw, rc->data_size * sizeof(float), cudaMemcpyDeviceToHost,
+                              rc->ctx->stream));
+    CTBB_CUDA(cudaStreamSynchronize(rc->ctx->stream));
+    return CTBB_OK;
+}
+
 extern "C" ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host) {
     clear_error();
     if (!rc || !ssm) return fail(CTBB_ERR_INVALID_ARG, "null argument");
@@ -368,6 +378,14 @@ extern "C" ctbb_status ctbb_gpu_recon_get_volume_f64(ctbb_recon* rc, double* vol
     CTBB_CUDA(cudaMemcpyAsync(vol_host, rc->d_x64, rc->nvox * sizeof(double), cudaMemcpyDeviceToHost, st));
     CTBB_CUDA(cudaStreamSynchronize(st));
     return CTBB_OK;
+}
+
+extern "C" ctbb_status ctbb_gpu_recon_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* entries) {
+    clear_error();
+    if (!rc || !ssm || !entries) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    CTBB_TRY(check_pair(rc, ssm));
+    CTBB_CUDA(cudaSetDevice(rc->ctx->device));
+    return inrange_entries(rc, ssm, entries);
 }
 
 extern "C" ctbb_status ctbb_gpu_recon_refresh_residual(ctbb_recon* rc, const ctbb_ssm* ssm) {

@@ -17,7 +17,8 @@ widths are quoted at isocentre and converted to the detector
   cfg2  736 ch x 64 rows of 0.6 mm, in-plane FFS (2304 views/turn), pitch 1,
         4 turns, water phantom + 40 random ellipsoids, I0 per view in
         5e4..2e5, 512 x 512 x 64 at 0.6 mm, 30 cm FOV, edge-preserving with
-        delta = 5 HU (9.6e-4 cm^-1).
+        delta = 5 HU (9.6e-4 cm^-1) and lambda = 0.1 (the value of the
+        reference's resources/sample_prm.yaml; the benchmark names none).
   tiny, tiny_ffs, small, small_ffs, mid
         reduced geometries (few channels/rows/views, large voxels) that the
         reference program finishes in seconds: golden fixtures and parity
@@ -87,8 +88,23 @@ WORKLOADS = {
     "cfg2": dict(
         prm={**_BASE,
              **_scanner(736, 366.25, FAN_INC, 64, 0.06, 1152, True, 1.0, 4),
-             **_recon(512, 30.0, 0.06, 64, -3.0, "edge-preserving", 0.01, 9.6e-4, 10)},
+             **_recon(512, 30.0, 0.06, 64, -3.0, "edge-preserving", 0.1, 9.6e-4, 10)},
         phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+    ),
+    # cfg2's scanner, views, flying focal spot and penalty over the full 30 cm
+    # FOV at 128 x 128 (2.3 mm voxels) x 16 slices of 0.6 mm, two turns.
+    "cfg2_lite": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 64, 0.06, 1152, True, 1.0, 2),
+             **_recon(128, 30.0, 0.06, 16, -2.0, "edge-preserving", 0.1, 9.6e-4, 10)},
+        phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+    ),
+    # cfg1's scanner and penalty at 64 x 64 x 8 (3.9 mm voxels, 1 mm slices).
+    "cfg1_small": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 16, 0.12, 1152, False, 1.0, 3),
+             **_recon(64, 25.0, 0.1, 8, -1.5, "quadratic", 1e3, 0.005, 10)},
+        phantom=dict(n_ellipsoids=0, seed=0, i0_lo=1e5, i0_hi=1e5),
     ),
     # Reduced geometries (not in the benchmark): 48 channels covering the
     # 25 cm FOV, 4 rows of 1.5 cm, 96 (or 128 x 2 with FFS) views per turn.
@@ -148,7 +164,9 @@ def prm_text(prm: dict) -> str:
     for k in keys:
         v = prm[k]
         if isinstance(v, float):
-            v = repr(v)
+            v = repr(float(v))
+        elif hasattr(v, "item"):
+            v = v.item()
         lines.append(f"{k}: {v}")
     return "\n".join(lines) + "\n"
 

@@ -270,6 +270,7 @@ typedef struct ctbb_icd_opts {
     int32_t lattice;          /* grouped: in-plane spacing of the visiting order (0: auto) */
     int32_t compute_cost;     /* evaluate the FP64 cost after each iteration      */
     double stop_rel_change;   /* stop when |dcost|/cost < this (0: fixed count)   */
+    double relax;             /* grouped: step scale omega in (0, 2) (0: 1.0)     */
 } ctbb_icd_opts;
 
 typedef struct ctbb_iter_stats {
@@ -292,6 +293,8 @@ ctbb_status ctbb_gpu_recon_create(ctbb_ctx* ctx, const ctbb_geom_c* geom,
 void ctbb_gpu_recon_free(ctbb_recon* rc);
 ctbb_status ctbb_gpu_recon_set_raw(ctbb_recon* rc, const float* raw_host);
 ctbb_status ctbb_gpu_recon_set_raw_device(ctbb_recon* rc, const float* raw_dev);
+/* Copy the recon's raw data y back to the host. */
+ctbb_status ctbb_gpu_recon_get_raw(ctbb_recon* rc, float* raw_host);
 /* Device pointer of the recon's raw buffer (for the GPU projector). */
 float* ctbb_gpu_recon_raw_device(ctbb_recon* rc);
 /* Initial image (host, float [nz][ny][nx]); NULL -> zeros. Resets e = y - Ax. */
@@ -301,6 +304,9 @@ ctbb_status ctbb_gpu_recon_get_volume_f64(ctbb_recon* rc, double* vol_host);
 /* Run n_iter ICD iterations. */
 ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts* opts,
                                    int32_t n_iter, ctbb_iter_stats* stats);
+/* Sum over voxels inside the scanner FOV of the matrix entries whose sinogram
+ * index lies inside the scan (the entries one ICD iteration visits). */
+ctbb_status ctbb_gpu_recon_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* entries);
 /* Recompute e = y - Ax with FP64 accumulation. */
 ctbb_status ctbb_gpu_recon_refresh_residual(ctbb_recon* rc, const ctbb_ssm* ssm);
 /* FP64 cost of the current iterate (quadratic: 1/2|e|^2 + lambda/4 sum w dx^2;

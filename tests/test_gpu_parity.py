@@ -1,0 +1,198 @@
+"""GPU parity: the CUDA path (through the C ABI) against the reference's own
+outputs (golden fixtures) and the CPU oracle at larger sizes."""
+import os
+
+import numpy as np
+import pytest
+
+import ctbb_icd_b200 as C
+import oracle_util as O
+from ctbb_icd_b200 import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+MU_W = 0.192
+HU = MU_W / 1000.0  # cm^-1 per HU
+
+
+@pytest.fixture(scope="module", params=["small", "small_ffs", "mid"])
+def wl(request, tmp_path_factory):
+    d = str(tmp_path_factory.mktemp(request.param))
+    prm, rp = W.materialise(request.param, d)
+    data = C.load_raw(rp)
+    return request.param, rp, data, O.port_ssm(rp)
+
+
+# ---------------------------------------------------------------- SSM ----
+def test_ssm_matches_reference_matrix_bin(golden, ctx, tmp_path):
+    ssm = C.Ssm.generate(golden.rp, ctx, C.SSM_BOTH)
+    path = str(tmp_path / "matrix.bin")
+    ssm.export_reference(path)
+    m = O.read_matrix_bin(path, int(golden.rp.geom.nx * golden.rp.geom.ny))
+    assert np.array_equal(m.colptr, golden.colptr)
+    assert np.array_equal(m.idx, golden.idx)
+    assert np.array_equal(m.w.view(np.int32), golden.w.view(np.int32))
+    info = ssm.info()
+    assert info.nnz == golden.colptr[-1] and info.ffs == int(golden.rp.geom.Phiffs)
+
+
+def test_ssm_matches_port(wl, ctx):
+    name, rp, data, ref = wl
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
+    assert ssm.info().nnz == ref.nnz
+    ncol = int(rp.geom.nx * rp.geom.ny)
+    for c in list(range(0, ncol, max(1, ncol // 97))) + [ncol - 1]:
+        idx, w = ssm.column(c)
+        ri, rw = ref.column(c)
+        assert np.array_equal(idx, ri), (name, c)
+        assert np.array_equal(w.view(np.int32), rw.view(np.int32)), (name, c)
+
+
+def test_ssm_fp16_weights_are_rounded_fp32(ctx, golden):
+    s32 = C.Ssm.generate(golden.rp, ctx, C.SSM_FP32)
+    s16 = C.Ssm.generate(golden.rp, ctx, C.SSM_FP16)
+    for c in (0, 37, 100):
+        i32, w32 = s32.column(c)
+        i16, w16 = s16.column(c)
+        assert np.array_equal(i32, i16)
+        assert np.array_equal(w16, w32.astype(np.float16).astype(np.float32))
+
+
+def test_ssm_import_reference_round_trip(golden, ctx, tmp_path):
+    path = str(tmp_path / "in.bin")
+    with open(path, "wb") as f:
+        for c in range(len(golden.colptr) - 1):
+            b, e = golden.colptr[c], golden.colptr[c + 1]
+            np.array([e - b], np.uint64).tofile(f)
+            rec = np.empty((e - b, 2), np.int32)
+            rec[:, 0] = golden.idx[b:e]
+            rec[:, 1] = golden.w[b:e].view(np.int32)
+            rec.tofile(f)
+    ssm = C.Ssm.import_reference(golden.rp, path, ctx)
+    out = str(tmp_path / "out.bin")
+    ssm.export_reference(out)
+    assert open(path, "rb").read() == open(out, "rb").read()
+
+
+def test_ssm_import_rejects_corrupt_file(golden, ctx, tmp_path):
+    path = str(tmp_path / "bad.bin")
+    np.array([5], np.uint64).tofile(path)  # claims 5 entries, holds none
+    with pytest.raises(C.CtbbError) as e:
+        C.Ssm.import_reference(golden.rp, path, ctx)
+    assert e.value.status == 10
+
+
+# ----------------------------------------------------------- rotation ----
+def test_rotate_matches_reference_final_image(golden, ctx):
+    d = C.CtData(recon_volume=golden.iterations[-1].astype(np.float32), tube_angles=golden.data.tube_angles,
+                 slice_indices=golden.data.slice_indices)
+    C.rotate_slices_rotating2fixed(golden.rp, d, ctx)
+    assert np.array_equal(d.recon_volume.view(np.int32), golden.final.view(np.int32))
+
+
+def test_rotate_both_directions_match_port(wl, ctx):
+    name, rp, data, _ = wl
+    vol = np.random.default_rng(3).random(rp.shape, dtype=np.float32)
+    for direction, fn in ((-1, C.rotate_slices_rotating2fixed), (1, C.rotate_slices_fixed2rotating)):
+        d = C.CtData(recon_volume=vol.copy(), tube_angles=data.tube_angles, slice_indices=data.slice_indices)
+        fn(rp, d, ctx)
+        ref = O.port_rotate(rp, data.tube_angles, data.slice_indices, vol, direction)
+        assert np.array_equal(d.recon_volume.view(np.int32), ref.view(np.int32)), (name, direction)
+
+
+# ------------------------------------------------------ sequential ICD ----
+def test_sequential_icd_matches_reference_iterations(golden, ctx):
+    ssm = C.Ssm.generate(golden.rp, ctx, C.SSM_FP32)
+    rc = C.Recon(golden.rp, golden.data.slice_indices, ctx)
+    rc.set_raw(golden.raw)
+    rc.set_volume(ssm, None)
+    opts = C.icd_opts(mode=C.ICD_SEQUENTIAL)
+    for it in range(golden.iterations.shape[0] - 1):
+        rc.iterate(ssm, 1, opts)
+        x = rc.volume_f64()
+        ref = golden.iterations[it + 1]
+        rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+        assert rel < 1e-5 and np.abs(x - ref).max() <= 1e-5 * np.abs(ref).max(), (it, rel)
+        assert rel < 1e-12, (it, rel)  # only the alpha/beta summation order differs
+
+
+def test_sequential_icd_matches_port(wl, ctx):
+    name, rp, data, ref = wl
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    dumps, _, _ = O.port_icd(rp, data.slice_indices, data.raw, ref, 3)
+    for it in range(3):
+        rc.iterate(ssm, 1, C.icd_opts(mode=C.ICD_SEQUENTIAL))
+        x = rc.volume_f64()
+        rel = np.linalg.norm(x - dumps[it]) / np.linalg.norm(dumps[it])
+        assert rel < 1e-10, (name, it, rel)
+
+
+def test_pipeline_stage_functions_reproduce_reference_output(golden, ctx):
+    rp = C.configure_recon_params(golden.prm_path)
+    data = C.load_raw(rp)
+    C.initialize_recon_volume(rp, data)
+    C.generate_system_matrix(rp, data, ctx)
+    C.icd_iteration(rp, data, ctx)
+    C.rotate_slices_rotating2fixed(rp, data, ctx)
+    out = C.clean_up(rp, data)
+    img = np.fromfile(out, np.float32).reshape(rp.shape)
+    # FP64 iterates agree to ~1e-15; a float cast may flip one ulp.
+    assert np.allclose(img, golden.final, rtol=1e-6, atol=1e-7)
+
+
+# ------------------------------------------------ residual, cost, synth ----
+def test_refresh_residual_and_cost_match_port(wl, ctx):
+    name, rp, data, ref = wl
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
+    rng = np.random.default_rng(7)
+    x0 = (0.2 * rng.random(rp.shape)).astype(np.float32)
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, x0)
+    cost_ref, _, _ = O.port_cost(rp, data.slice_indices, data.raw, ref, x0.astype(np.float64))
+    assert abs(rc.cost() - cost_ref) <= 1e-9 * abs(cost_ref), name
+    # grouped representation: e = y - A x in FP32 after an FP64 refresh
+    rc.iterate(ssm, 0, C.icd_opts(mode=C.ICD_GROUPED))
+    rc.refresh_residual(ssm)
+    assert abs(rc.cost() - cost_ref) <= 1e-5 * abs(cost_ref), name
+
+
+def test_gpu_projector_matches_cpu(ctx, tmp_path):
+    import ctypes
+
+    prm, rp = W.materialise("small_ffs", str(tmp_path), raw=False)
+    spec = W.phantom_spec("small_ffs")
+    cpu = O.port_synth(rp, spec)
+    sl = C.slice_tables(rp)
+    rc = C.Recon(rp, sl.slice_indices, ctx)
+    C.check(C.lib().ctbb_gpu_synth_raw(ctx.handle, ctypes.byref(rp.geom), ctypes.byref(spec),
+                                       ctypes.c_void_p(rc.raw_device_ptr())))
+    gpu = rc.raw()
+    diff = np.abs(gpu - cpu)
+    # libm rounding (exp/log/lgamma) can move a Poisson draw by one count in rare rays
+    assert np.mean(diff == 0) > 0.99
+    assert diff.max() < 0.05
+
+
+# ------------------------------------------------------- grouped ICD ----
+@pytest.mark.parametrize("weights", [C.SSM_FP32, C.SSM_FP16])
+def test_grouped_icd_reaches_converged_cost(ctx, tmp_path, weights):
+    prm, rp = W.materialise("small", str(tmp_path))
+    data = C.load_raw(rp)
+    ref = O.port_ssm(rp)
+    # Converged plain sequential ICD on the CPU oracle.
+    _, x_ref, _ = O.port_icd(rp, data.slice_indices, data.raw, ref, 150)
+    cost_ref = O.port_cost(rp, data.slice_indices, data.raw, ref, x_ref)[0]
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_BOTH)
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    rc.iterate(ssm, 150, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5))
+    x = rc.volume_f64()
+    cost = O.port_cost(rp, data.slice_indices, data.raw, ref, x)[0]
+    rmse_hu = np.sqrt(np.mean((x - x_ref) ** 2)) / HU
+    assert rmse_hu <= 0.5, rmse_hu
+    assert cost <= cost_ref * (1 + 1e-6), (cost, cost_ref)
