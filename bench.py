@@ -38,6 +38,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 WORKLOAD = "cfg2"
+WORKLOAD_TEXT = ("grouped ICD, 512x512x64 @ 0.6 mm, 30 cm FOV, 736 ch x 64 rows, in-plane FFS, "
+                 "2304 views/turn, 4 turns (9216 views), edge-preserving (delta 9.6e-4, lambda 0.1)")
 HBM_FALLBACK_GBS = 6650.0
 
 
@@ -111,11 +113,11 @@ class ClockSampler:
 # --------------------------------------------------------------------------
 # Our arm
 # --------------------------------------------------------------------------
-def setup_workload(ctx, workdir, seed, weights):
+def setup_workload(ctx, workdir, seed, weights, name=WORKLOAD):
     import ctbb_icd_b200 as C
     from ctbb_icd_b200 import workloads as W
 
-    w = W.workload(WORKLOAD)
+    w = W.workload(name)
     w["phantom"]["seed"] = seed
     prm = w["prm"]
     prm.update(sinogram_path=os.path.join(workdir, "raw.bin"), output_dir=workdir, output_file="out.img")
@@ -145,7 +147,8 @@ def run_ours(args, rank, world, dist):
     weights_fmt = C.SSM_FP16 if args.weights == "fp16" else C.SSM_FP32
     workdir = tempfile.mkdtemp(prefix="ctbb_bench_")
     t0 = time.time()
-    rp, tables, rc, ssm = setup_workload(ctx, workdir, seed=rank, weights=C.SSM_BOTH if args.e2e else weights_fmt)
+    rp, tables, rc, ssm = setup_workload(ctx, workdir, seed=rank, weights=C.SSM_BOTH if args.e2e else weights_fmt,
+                                         name=args.workload)
     setup_s = time.time() - t0
     info = ssm.info()
     opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice)
@@ -210,8 +213,7 @@ def run_ours(args, rank, world, dist):
             "dtype": "f32",
             "data": "synthetic (seeded phantom: water + 6 inserts + 40 ellipsoids, Poisson noise, GPU projector)",
             "config": {
-                "workload": "grouped ICD, 512x512x64 @ 0.6 mm, 30 cm FOV, 736 ch x 64 rows, in-plane FFS, "
-                            "2304 views/turn, 4 turns (9216 views), edge-preserving (delta 9.6e-4)",
+                "workload": WORKLOAD_TEXT if args.workload == WORKLOAD else args.workload,
                 "weights": args.weights, "error_sinogram": "fp32", "voxels": nvox,
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
@@ -453,6 +455,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--weights", choices=["fp16", "fp32"], default="fp16")
+    ap.add_argument("--workload", default=WORKLOAD,
+                    help="workload name from ctbb_icd_b200.workloads (the benchmark is cfg2)")
     ap.add_argument("--warps", type=int, default=0, help="warps in flight (0: auto)")
     ap.add_argument("--lattice", type=int, default=0)
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")

@@ -99,6 +99,18 @@ WORKLOADS = {
              **_recon(128, 30.0, 0.06, 16, -2.0, "edge-preserving", 0.1, 9.6e-4, 10)},
         phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
     ),
+    # cfg2's voxel size, detector, views and flying focal spot on the central
+    # 7.5 cm (128 x 128 x 16) of the FOV over 1.5 turns: the per-voxel matrix
+    # footprint and sinogram access pattern of cfg2 at 1/64 of its volume, for
+    # kernel profiling (the object extends past this FOV, so its images are
+    # not meaningful reconstructions).
+    "cfg2_center": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 64, 0.06, 1152, True, 1.0, 1),
+             "Readings": 3456,
+             **_recon(128, 7.5, 0.06, 16, -1.8, "edge-preserving", 0.1, 9.6e-4, 10)},
+        phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+    ),
     # cfg1's scanner and penalty at 64 x 64 x 8 (3.9 mm voxels, 1 mm slices).
     "cfg1_small": dict(
         prm={**_BASE,

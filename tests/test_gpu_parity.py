@@ -178,21 +178,37 @@ def test_gpu_projector_matches_cpu(ctx, tmp_path):
 
 
 # ------------------------------------------------------- grouped ICD ----
-@pytest.mark.parametrize("weights", [C.SSM_FP32, C.SSM_FP16])
-def test_grouped_icd_reaches_converged_cost(ctx, tmp_path, weights):
-    prm, rp = W.materialise("small", str(tmp_path))
+@pytest.fixture(scope="module")
+def converged_cfg1_small(ctx, tmp_path_factory):
+    """cfg1's scanner and quadratic penalty at 64 x 64 x 8: the converged
+    plain sequential-order ICD image (30 iterations; iterations 20-60 agree
+    to < 0.02 HU) and its FP64 cost."""
+    prm, rp = W.materialise("cfg1_small", str(tmp_path_factory.mktemp("cfg1_small")))
     data = C.load_raw(rp)
-    ref = O.port_ssm(rp)
-    # Converged plain sequential ICD on the CPU oracle.
-    _, x_ref, _ = O.port_icd(rp, data.slice_indices, data.raw, ref, 150)
-    cost_ref = O.port_cost(rp, data.slice_indices, data.raw, ref, x_ref)[0]
     ssm = C.Ssm.generate(rp, ctx, C.SSM_BOTH)
     rc = C.Recon(rp, data.slice_indices, ctx)
     rc.set_raw(data.raw)
     rc.set_volume(ssm, None)
-    rc.iterate(ssm, 150, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5))
+    rc.iterate(ssm, 30, C.icd_opts(mode=C.ICD_SEQUENTIAL))
+    x_ref = rc.volume_f64()
+    cost_ref = rc.cost()
+    rc.free()
+    return rp, data, ssm, x_ref, cost_ref
+
+
+@pytest.mark.parametrize("weights", [C.SSM_FP32, C.SSM_FP16])
+def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights):
+    rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    costs = []
+    for _ in range(6):
+        rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5))
+        rc.refresh_residual(ssm)
+        costs.append(rc.cost())
     x = rc.volume_f64()
-    cost = O.port_cost(rp, data.slice_indices, data.raw, ref, x)[0]
     rmse_hu = np.sqrt(np.mean((x - x_ref) ** 2)) / HU
+    assert all(b <= a * (1 + 1e-9) for a, b in zip(costs, costs[1:])), costs
     assert rmse_hu <= 0.5, rmse_hu
-    assert cost <= cost_ref * (1 + 1e-6), (cost, cost_ref)
+    assert abs(costs[-1] - cost_ref) <= 1e-6 * abs(cost_ref), (costs[-1], cost_ref)
