@@ -152,6 +152,7 @@ PROTOTYPES = {
     "ctbb_gpu_icd": (_I, [_P, _P, _PG, _PU, _PF, _PF, C.POINTER(IcdOpts), C.POINTER(IterStats)]),
     "ctbb_gpu_rotate": (_I, [_P, _PG, _PD, _PU, _PF, _I]),
     "ctbb_gpu_rotate_device": (_I, [_P, _PG, _PD, _PU, _P, _P, _I]),
+    "ctbb_gpu_rotate_device_noalloc": (_I, [_P, _PG, _PD, _PU, _P, _P, _I]),
 }
 
 _lib = None

@@ -14,6 +14,7 @@
 #include <math.h>
 
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "gpu_internal.h"
@@ -109,6 +110,87 @@ extern "C" ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* 
     if (in_dev == out_dev) return fail(CTBB_ERR_INVALID_ARG, "in and out must not alias");
     CTBB_CUDA(cudaSetDevice(ctx->device));
     return rotate_device(ctx, *geom, tube_angles_deg, slice_indices, in_dev, out_dev, direction);
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of ctbb_gpu_rotate_device.
+//
+// Some callers cannot let a library call cudaMalloc: applications that hand
+// out all device memory from their own pool up front (so a stray allocation
+// could fail or fragment it), real-time reconstruction loops that must not
+// hit the allocator's implicit synchronisation, and embedders that run the
+// rotation between other work without wanting the driver to grow the
+// process's footprint. For them the per-slice cos/sin table, the only scratch
+// the rotation kernel needs, lives in this fixed device array instead of a
+// cudaMalloc'd buffer.
+//
+// The array is a file-scope __device__ symbol, so every GPU that loads this
+// library holds it (2 * kNoAllocMaxSlices doubles, 128 KB) until the process
+// exits. Host code only knows the symbol's host-side shadow, so the device
+// address is looked up with cudaGetSymbolAddress once per device, with that
+// device current, the first time the entry point runs on it.
+// ---------------------------------------------------------------------------
+namespace {
+
+constexpr uint64_t kNoAllocMaxSlices = 8192;
+static __device__ __align__(256) double g_rotate_scratch[2 * kNoAllocMaxSlices];
+
+constexpr int kMaxDevices = 64;
+std::mutex g_scratch_mutex;
+double* g_scratch_addr[kMaxDevices] = {};
+
+// Device address of g_rotate_scratch on `device` (which must be current).
+ctbb_status scratch_address(int device, double** out) {
+    using namespace ctbb;
+    if (device < 0 || device >= kMaxDevices) return fail(CTBB_ERR_INVALID_ARG, "device index %d too large", device);
+    std::lock_guard<std::mutex> lock(g_scratch_mutex);
+    if (!g_scratch_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_rotate_scratch);
+        if (e != cudaSuccess)
+            return fail(CTBB_ERR_CUDA, "cudaGetSymbolAddress(g_rotate_scratch): %s", cudaGetErrorString(e));
+        g_scratch_addr[device] = (double*)p;
+    }
+    *out = g_scratch_addr[device];
+    return CTBB_OK;
+}
+
+}  // namespace
+
+extern "C" ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                                                      const double* tube_angles_deg, const uint64_t* slice_indices,
+                                                      const float* in_dev, float* out_dev, int32_t direction) {
+    clear_error();
+    if (!ctx || !geom || !tube_angles_deg || !slice_indices || !in_dev || !out_dev)
+        return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (in_dev == out_dev) return fail(CTBB_ERR_INVALID_ARG, "in and out must not alias");
+    if (direction != CTBB_ROTATE_FIXED2ROTATING && direction != CTBB_ROTATE_ROTATING2FIXED)
+        return fail(CTBB_ERR_INVALID_ARG, "direction must be +1 or -1");
+    if (geom->num_voxels_z > kNoAllocMaxSlices)
+        return fail(CTBB_ERR_INVALID_ARG,
+                    "ctbb_gpu_rotate_device_noalloc handles at most %llu slices (got %llu); use ctbb_gpu_rotate_device",
+                    (unsigned long long)kNoAllocMaxSlices, (unsigned long long)geom->num_voxels_z);
+    if (geom->num_voxels_x != geom->num_voxels_y)
+        return fail(CTBB_ERR_INVALID_ARG, "slice rotation needs square slices (rotate_slices.cpp:128)");
+    CTBB_CUDA(cudaSetDevice(ctx->device));
+    double* d_cs = nullptr;
+    CTBB_TRY(scratch_address(ctx->device, &d_cs));
+    // Every slice's entries are rewritten below, so nothing left by an
+    // earlier call needs clearing.
+    std::vector<double> cs;
+    CTBB_TRY(angles(*geom, tube_angles_deg, slice_indices, direction, cs));
+    if (cs.empty()) return CTBB_OK;
+    cudaStream_t st = ctx->stream;
+    CTBB_CUDA(cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    const ctbb_geom_c& g = *geom;
+    const uint64_t n = g.num_voxels_x * g.num_voxels_y * g.num_voxels_z;
+    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
+    rotate_kernel<<<grid, 256, 0, st>>>(in_dev, out_dev, (int)g.num_voxels_x, (int)g.num_voxels_y,
+                                        (int)g.num_voxels_z, (int)g.nx, (int)g.ny, (int)g.num_voxels_y, d_cs,
+                                        g.center_voxel_x, g.center_voxel_y);
+    CTBB_CUDA(cudaGetLastError());
+    CTBB_CUDA(cudaStreamSynchronize(st));
+    return CTBB_OK;
 }
 
 extern "C" ctbb_status ctbb_gpu_rotate(ctbb_ctx* ctx, const ctbb_geom_c* geom, const double* tube_angles_deg,

@@ -341,6 +341,31 @@ ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* geom,
                                    const double* tube_angles_deg, const uint64_t* slice_indices,
                                    const float* in_dev, float* out_dev, int32_t direction);
 
+/*
+ * ctbb_gpu_rotate_device without any device allocation. It has no
+ * counterpart in the reference (whose rotation runs on the host).
+ *
+ * For callers that must not have a library call cudaMalloc/cudaFree: code
+ * that carves all device memory out of its own pool at start-up, latency-
+ * bound loops that cannot afford the allocator's implicit synchronisation,
+ * or hosts that cap the process's device footprint. The only scratch the
+ * rotation needs, the per-slice cos/sin table, is kept in a fixed device
+ * array of 2 x 8192 doubles (128 KB) that every GPU loading this library
+ * holds until the process exits; volumes of more than 8192 slices are
+ * rejected with CTBB_ERR_INVALID_ARG. Input and output stay caller-owned
+ * device buffers and give the same result as ctbb_gpu_rotate_device.
+ *
+ * The first call on each device looks up the array's device address, so
+ * make that first call before any stream capture starts. All calls share the
+ * one array: calls whose work overlaps on the GPU (other host threads or
+ * streams of the same device) race on it. Each call rewrites the entries it
+ * uses, so nothing left by an earlier call leaks into a later one.
+ */
+ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geom,
+                                           const double* tube_angles_deg,
+                                           const uint64_t* slice_indices, const float* in_dev,
+                                           float* out_dev, int32_t direction);
+
 #ifdef __cplusplus
 }
 #endif
