@@ -60,13 +60,16 @@ class ClockSampler:
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, gpu_index: int):
+    def __init__(self, gpu_index: int, enabled: bool = True):
         self.gpu = gpu_index
+        self.enabled = enabled
         self.proc = None
         self.lines = []
         self.thread = None
 
     def start(self):
+        if not self.enabled:
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -143,7 +146,11 @@ def run_ours(args, rank, world, dist):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     torch_stream = torch.cuda.Stream(device=local)
-    ctx = C.Context(local, ctypes.c_void_p(torch_stream.cuda_stream))
+    if args.own_stream:
+        ctx = C.Context(local)
+        torch_stream = torch.cuda.ExternalStream(ctx.stream, device=local)
+    else:
+        ctx = C.Context(local, ctypes.c_void_p(torch_stream.cuda_stream))
     weights_fmt = C.SSM_FP16 if args.weights == "fp16" else C.SSM_FP32
     workdir = tempfile.mkdtemp(prefix="ctbb_bench_")
     t0 = time.time()
@@ -162,7 +169,7 @@ def run_ours(args, rank, world, dist):
     w_bytes = 2 if weights_fmt == C.SSM_FP16 else 4
     b_iter = 8.0 * entries + (4 + w_bytes) * float(info.nnz) + 8.0 * nvox
 
-    clocks = ClockSampler(local)
+    clocks = ClockSampler(local, enabled=args.clocks)
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
@@ -463,6 +470,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=10, help="ICD iterations per drop-in call")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-clocks", dest="clocks", action="store_false", help="skip nvidia-smi clock sampling")
+    ap.add_argument("--own-stream", action="store_true", help="run on the library's own stream")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -76,6 +76,11 @@ struct ctbb_recon {
     // Sum over voxels inside the FOV of in-range matrix entries (cached per matrix).
     const ctbb_ssm* entries_ssm = nullptr;
     double entries = 0.0;
+    // Grouped-mode visiting order: packed (column * nz + slice) per item,
+    // built once per lattice spacing.
+    uint32_t* d_order = nullptr;
+    uint64_t n_order = 0;
+    int order_P = 0;
 };
 
 namespace ctbb {

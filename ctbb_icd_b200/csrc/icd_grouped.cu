@@ -16,16 +16,26 @@
 //     reference's bisection bracket;
 //   * scatter: e -= delta a with fire-and-forget L2 reductions (red.global.add).
 //
-// Visiting order (the "groups"): voxels are enumerated lattice by lattice.
-// A lattice is every P-th column in x and y at offset (a, b) and every Q-th
-// slice at residue r; lattice offsets are visited in a scrambled order. The
-// items in flight at any moment (about `warps_in_flight` of them) are
-// consecutive in this order, so they are P columns apart in-plane and Q slices
-// apart in z: their footprints overlap only where two voxels are collinear
-// with the source, and never through the penalty neighbourhood. Footprints of
-// a whole lattice are not disjoint (any two voxels of one slice share rays at
-// the views where they line up with the source), so updates of one lattice
-// meet in the red.global.add scatter rather than being ordered.
+// Visiting order (the "groups"). A voxel update touches ~2 short runs of
+// detector rows per view, each costing a whole 32-byte sector, so what bounds
+// the kernel is DRAM sectors, not bytes. The voxels whose runs share sectors
+// are the ones at the same physical (x, y) position in different slices:
+// they project to the same channels and to neighbouring rows. With rotating
+// slices (Xu & Tsui), that physical position is a different column index in
+// every slice, so the order is built from physical positions:
+//
+//   key = (lattice offset, slice parity, lattice cell, slice)
+//
+// where the cell is the voxel's centre rotated into the fixed frame (by the
+// tube angle of the slice's central view) and snapped to the grid, lattices
+// are every P-th cell in x and y (offsets visited in a scrambled order, cells
+// along a golden-ratio stride), and slices of one parity are consecutive. The
+// ~`warps_in_flight` items in flight at any moment are then ~W/(nz/2) cells,
+// P cells apart, each with its stack of every-other slice: the stack shares
+// sectors (its z-profiles are disjoint, so it is nearly uncoupled), the cells
+// are far apart and never penalty neighbours. Footprints of a lattice still
+// overlap where voxels line up with the source, so the scatter is an L2
+// reduction rather than ordered stores.
 //
 // The warp count in flight bounds how stale a gather can be: with W warps
 // and a voxel footprint crossing ~T voxels per ray, about T*W/N voxels of a
@@ -33,6 +43,8 @@
 #include <math.h>
 
 #include <algorithm>
+#include <cub/cub.cuh>
+#include <vector>
 
 #include "gpu_internal.h"
 
@@ -40,8 +52,7 @@ namespace {
 
 struct GParams {
     int nx, ny, nz, nch, nr, nvsm, readings, penalty;
-    int P, Q, mx, my, kq, n_offsets, stride, pstride;
-    uint64_t n_items, per_offset, per_residue, nvsm1;
+    uint64_t n_items, nvsm1;
     float lambda, delta;
     double relax;  // step scale applied to the exact 1-D update before the positivity clamp
     double cvx, cvy, vx, vy, fov_limit;
@@ -73,7 +84,8 @@ __device__ __forceinline__ float ldw<__half>(const __half* w, int64_t m) {
 }
 
 template <class WT>
-__global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64_t* __restrict__ colptr,
+__global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint32_t* __restrict__ order,
+                                                          const int64_t* __restrict__ colptr,
                                                           const uint32_t* __restrict__ vptr,
                                                           const int32_t* __restrict__ idx,
                                                           const WT* __restrict__ w, const int32_t* __restrict__ start,
@@ -98,24 +110,9 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64
         if (lane == 0) item = atomicAdd(queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= P.n_items) break;
-        // Decode the visiting order: offset, slice residue, lattice point, slice.
-        const int o = (int)(item / P.per_offset);
-        uint64_t rem = item % P.per_offset;
-        const int r = (int)(rem / P.per_residue);
-        rem %= P.per_residue;
-        const int pt = (int)(rem / P.kq);
-        const int kk = (int)(rem % P.kq);
-        const int os = (int)(((uint64_t)o * P.stride) % P.n_offsets);
-        // Golden-ratio stride over the lattice points spreads consecutive
-        // items (and hence the items in flight) over the whole slice.
-        const int ps = (int)(((uint64_t)pt * P.pstride) % (uint64_t)(P.mx * P.my));
-        const int i = os % P.P + P.P * (ps % P.mx);
-        const int j = os / P.P + P.P * (ps / P.mx);
-        const int k = r + P.Q * kk;
-        if (i >= P.nx || j >= P.ny || k >= P.nz) continue;
-        const double xx = (i - P.cvx) * P.vx, yy = (j - P.cvy) * P.vy;
-        if (!(xx * xx + yy * yy < P.fov_limit)) continue;
-        const uint64_t col = (uint64_t)i + (uint64_t)P.nx * j;
+        const uint32_t packed = __ldg(order + item);
+        const uint64_t col = packed / (uint32_t)P.nz;
+        const int k = (int)(packed % (uint32_t)P.nz);
         const int64_t q = (int64_t)col + (int64_t)ncol * k;
         const int s = start[k];
         const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
@@ -216,6 +213,40 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const int64
     }
 }
 
+// Sort keys of the visiting order (see the file comment); voxels outside the
+// scanner FOV (icd_iteration.cpp:181) get the largest key and are dropped.
+struct OrderParams {
+    int nx, ny, nz, P, Q, margin, lx, stride, gstride;
+    uint64_t lt;
+    double cvx, cvy, vx, vy, fov_limit;
+};
+
+__global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, uint64_t* __restrict__ keys,
+                                  uint32_t* __restrict__ vals) {
+    const uint64_t ncol = (uint64_t)O.nx * O.ny, n = ncol * O.nz;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t / ncol);
+        const uint64_t col = t % ncol;
+        const int i = (int)(col % O.nx), j = (int)(col / O.nx);
+        vals[t] = (uint32_t)(col * O.nz + k);
+        const double xx = (i - O.cvx) * O.vx, yy = (j - O.cvy) * O.vy;
+        if (!(xx * xx + yy * yy < O.fov_limit)) {
+            keys[t] = ~0ull;
+            continue;
+        }
+        // Voxel centre in the fixed frame, in voxel units, snapped to the grid.
+        const double c = cs[2 * k], s = cs[2 * k + 1];
+        const double px = c * (i - O.cvx) - s * (j - O.cvy) + O.cvx;
+        const double py = s * (i - O.cvx) + c * (j - O.cvy) + O.cvy;
+        const int a = (int)llrint(px) + O.margin, b = (int)llrint(py) + O.margin;
+        const int off = (a % O.P) + O.P * (b % O.P);
+        const uint64_t rank_o = ((uint64_t)off * O.stride) % (uint64_t)(O.P * O.P);
+        const uint64_t cell = (uint64_t)(a / O.P) + (uint64_t)O.lx * (uint64_t)(b / O.P);
+        const uint64_t rank_c = (cell * O.gstride) % O.lt;
+        keys[t] = ((rank_o * O.Q + (uint64_t)(k % O.Q)) * O.lt + rank_c) * (uint64_t)O.nz + (uint64_t)k;
+    }
+}
+
 // Sum of in-range entries over (column inside the FOV, slice): the unit of
 // work of one iteration. One warp per column.
 __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uint32_t* __restrict__ vptr,
@@ -241,6 +272,21 @@ __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uin
     }
 }
 
+int gcd(int a, int b) {
+    while (b) {
+        const int t = a % b;
+        a = b;
+        b = t;
+    }
+    return a;
+}
+
+int coprime_near(int target, int n) {
+    int s = std::max(1, target);
+    while (n > 1 && gcd(s, n) != 1) ++s;
+    return s;
+}
+
 GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o) {
     const ctbb_geom_c& g = rc->geom;
     GParams P;
@@ -253,32 +299,7 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     P.nvsm1 = ssm->nvsm + 1;
     P.readings = (int)g.Readings;
     P.penalty = g.penalty;
-    P.P = o.lattice > 0 ? o.lattice : (P.nx >= 256 ? 16 : (P.nx >= 64 ? 8 : 4));
-    P.P = std::min(P.P, std::max(P.nx, P.ny));
-    P.Q = P.nz >= 2 ? 2 : 1;
-    P.mx = (P.nx + P.P - 1) / P.P;
-    P.my = (P.ny + P.P - 1) / P.P;
-    P.kq = (P.nz + P.Q - 1) / P.Q;
-    P.n_offsets = P.P * P.P;
-    // Stride coprime with P*P scrambles the order of lattice offsets.
-    int stride = P.n_offsets / 2 + 1;
-    auto gcd = [](int a, int b) {
-        while (b) {
-            const int t = a % b;
-            a = b;
-            b = t;
-        }
-        return a;
-    };
-    while (gcd(stride, P.n_offsets) != 1) ++stride;
-    P.stride = stride;
-    const int npts = P.mx * P.my;
-    int ps = std::max(1, (int)(0.6180339887 * npts));
-    while (npts > 1 && gcd(ps, npts) != 1) ++ps;
-    P.pstride = ps;
-    P.per_residue = (uint64_t)P.mx * P.my * P.kq;
-    P.per_offset = P.per_residue * P.Q;
-    P.n_items = P.per_offset * P.n_offsets;
+    P.n_items = rc->n_order;
     P.lambda = (float)g.lambda;
     P.delta = (float)g.delta;
     P.relax = (o.relax > 0.0 && o.relax < 2.0) ? o.relax : 1.0;
@@ -287,10 +308,114 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     P.vx = g.voxel_size_x;
     P.vy = g.voxel_size_y;
     P.fov_limit = (g.acquisition_fov / 2.0) * (g.acquisition_fov / 2.0);
-
     return P;
 }
 
+int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o) {
+    const int nx = (int)rc->geom.num_voxels_x;
+    int P = o.lattice > 0 ? o.lattice : (nx >= 256 ? 16 : (nx >= 64 ? 8 : 4));
+    return std::max(1, std::min(P, nx));
+}
+
+// Build (or reuse) the visiting order for lattice spacing P_lat.
+ctbb_status build_order(ctbb_recon* rc, int P_lat) {
+    using namespace ctbb;
+    if (rc->d_order && rc->order_P == P_lat) return CTBB_OK;
+    const ctbb_geom_c& g = rc->geom;
+    ctbb_ctx* ctx = rc->ctx;
+    cudaStream_t st = ctx->stream;
+    const uint64_t ncol = g.num_voxels_x * g.num_voxels_y, n = ncol * g.num_voxels_z;
+    if (n >= (1ull << 32)) return fail(CTBB_ERR_INVALID_ARG, "volume too large for the 32-bit visiting order");
+    // Rotation of each slice's frame: the tube angle of its central view.
+    std::vector<double> cs(2 * g.num_voxels_z);
+    const double PI = 3.141592653589793238;
+    for (uint64_t k = 0; k < g.num_voxels_z; ++k) {
+        const double deg = fmod((360.0 / g.num_views_per_turn) * (double)rc->slice_indices[k], 360.0);
+        cs[2 * k] = cos(deg * PI / 180.0);
+        cs[2 * k + 1] = sin(deg * PI / 180.0);
+    }
+    OrderParams O;
+    O.nx = (int)g.num_voxels_x;
+    O.ny = (int)g.num_voxels_y;
+    O.nz = (int)g.num_voxels_z;
+    O.P = P_lat;
+    O.Q = O.nz >= 2 ? 2 : 1;
+    O.margin = P_lat * ((std::max(O.nx, O.ny) + P_lat - 1) / P_lat);
+    O.lx = (O.nx + 2 * O.margin + P_lat - 1) / P_lat;
+    const int ly = (O.ny + 2 * O.margin + P_lat - 1) / P_lat;
+    O.lt = (uint64_t)O.lx * ly;
+    O.stride = coprime_near(P_lat * P_lat / 2 + 1, P_lat * P_lat);
+    O.gstride = coprime_near((int)(0.6180339887 * (double)O.lt), (int)O.lt);
+    O.cvx = g.center_voxel_x;
+    O.cvy = g.center_voxel_y;
+    O.vx = g.voxel_size_x;
+    O.vy = g.voxel_size_y;
+    O.fov_limit = (g.acquisition_fov / 2.0) * (g.acquisition_fov / 2.0);
+
+    double* d_cs = nullptr;
+    uint64_t *d_k0 = nullptr, *d_k1 = nullptr;
+    uint32_t *d_v0 = nullptr, *d_v1 = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    ctbb_status rcode = CTBB_OK;
+    auto cleanup = [&]() {
+        cudaFree(d_cs);
+        cudaFree(d_k0);
+        cudaFree(d_k1);
+        cudaFree(d_v0);
+        cudaFree(d_tmp);
+    };
+    cudaError_t e = cudaMalloc(&d_cs, cs.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_k0, n * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d_k1, n * sizeof(uint64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d_v0, n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMalloc(&d_v1, n * sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
+        order_keys_kernel<<<grid, 256, 0, st>>>(O, d_cs, d_k0, d_v0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, d_k0, d_k1, d_v0, d_v1, (int)n, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMalloc(&d_tmp, tmp_bytes);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_k0, d_k1, d_v0, d_v1, (int)n, 0, 64, st);
+    // Items outside the FOV sort last with key ~0; count the valid prefix.
+    uint64_t n_valid = n;
+    if (e == cudaSuccess) {
+        // Scan the sorted keys back from the end in chunks (few voxels lie
+        // outside the FOV, so this usually reads one chunk).
+        const uint64_t chunk = 1 << 20;
+        std::vector<uint64_t> buf;
+        uint64_t hi = n;
+        while (e == cudaSuccess && hi > 0) {
+            const uint64_t lo = hi > chunk ? hi - chunk : 0;
+            buf.resize(hi - lo);
+            e = cudaMemcpyAsync(buf.data(), d_k1 + lo, (hi - lo) * sizeof(uint64_t), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) break;
+            uint64_t p = hi - lo;
+            while (p > 0 && buf[p - 1] == ~0ull) --p;
+            n_valid = lo + p;
+            if (p > 0) break;
+            hi = lo;
+        }
+    }
+    if (e != cudaSuccess) {
+        rcode = fail(e == cudaErrorMemoryAllocation ? CTBB_ERR_OOM : CTBB_ERR_CUDA, "visiting order: %s",
+                     cudaGetErrorString(e));
+        cudaFree(d_v1);
+        cleanup();
+        return rcode;
+    }
+    cudaFree(rc->d_order);
+    rc->d_order = d_v1;
+    rc->n_order = n_valid;
+    rc->order_P = P_lat;
+    cleanup();
+    return CTBB_OK;
+}
 
 }  // namespace
 
@@ -327,6 +452,7 @@ int default_warps_in_flight(const ctbb_recon* rc) {
 
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
                                double* entries) {
+    CTBB_TRY(build_order(rc, lattice_spacing(rc, o)));
     const GParams P = make_params(rc, ssm, o);
     if (entries) CTBB_TRY(inrange_entries(rc, ssm, entries));
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
@@ -340,11 +466,13 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     CTBB_CUDA(cudaEventRecord(e0, st));
     const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
     if (wsel == CTBB_SSM_FP16)
-        icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, ssm->d_colptr, ssm->d_vptr, ssm->d_idx, ssm->d_w16,
-                                                           rc->d_start, rc->d_e32, rc->d_x32, ctx->d_queue);
+        icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, rc->d_order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
+                                                           ssm->d_w16, rc->d_start, rc->d_e32, rc->d_x32,
+                                                           ctx->d_queue);
     else
-        icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, ssm->d_colptr, ssm->d_vptr, ssm->d_idx, ssm->d_w32,
-                                                          rc->d_start, rc->d_e32, rc->d_x32, ctx->d_queue);
+        icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, rc->d_order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
+                                                          ssm->d_w32, rc->d_start, rc->d_e32, rc->d_x32,
+                                                          ctx->d_queue);
     CTBB_CUDA(cudaGetLastError());
     CTBB_CUDA(cudaEventRecord(e1, st));
     CTBB_CUDA(cudaEventSynchronize(e1));

@@ -293,6 +293,7 @@ extern "C" void ctbb_gpu_recon_free(ctbb_recon* rc) {
     cudaFree(rc->d_e32);
     cudaFree(rc->d_x64);
     cudaFree(rc->d_x32);
+    cudaFree(rc->d_order);
     delete rc;
 }
 
