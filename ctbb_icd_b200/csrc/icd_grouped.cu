@@ -22,19 +22,24 @@
 // are the ones at the same physical (x, y) position in different slices:
 // they project to the same channels and to neighbouring rows. With rotating
 // slices (Xu & Tsui), that physical position is a different column index in
-// every slice, so the order is built from physical positions:
+// every slice, so the order is built from physical positions: each voxel's
+// centre is rotated into the fixed frame (by the tube angle of its slice's
+// central view) and snapped to a grid cell; the plane is cut into T x T-cell
+// tiles, and
 //
-//   key = (lattice offset, slice parity, lattice cell, slice)
+//   key = (cell rank inside its tile, slice parity, tile, slice)
 //
-// where the cell is the voxel's centre rotated into the fixed frame (by the
-// tube angle of the slice's central view) and snapped to the grid, lattices
-// are every P-th cell in x and y (offsets visited in a scrambled order, cells
-// along a golden-ratio stride), and slices of one parity are consecutive. The
-// ~`warps_in_flight` items in flight at any moment are then ~W/(nz/2) cells,
-// P cells apart, each with its stack of every-other slice: the stack shares
-// sectors (its z-profiles are disjoint, so it is nearly uncoupled), the cells
-// are far apart and never penalty neighbours. Footprints of a lattice still
-// overlap where voxels line up with the source, so the scatter is an L2
+// with cells ranked along a serpentine raster. A "round" is one cell of every
+// tile (with one slice parity); the ~`warps_in_flight` items in flight are a
+// part of one round: stacks of every-other slice at the same relative cell of
+// many tiles, T cells apart. A stack shares sinogram sectors (its z-profiles
+// are disjoint, so it is nearly uncoupled); the next round moves every tile
+// to the neighbouring cell (or the other parity of the same cell), whose
+// footprint is still in L2, so the sinogram is streamed from DRAM a few times
+// per iteration instead of once per lattice pass. Neighbouring voxels are a
+// round apart, never in flight together as long as W is below a round, and
+// within a tile the sweep is the reference's raster-like order. Footprints
+// still overlap where voxels line up with the source, so the scatter is an L2
 // reduction rather than ordered stores.
 //
 // The warp count in flight bounds how stale a gather can be: with W warps
@@ -52,6 +57,7 @@ namespace {
 
 struct GParams {
     int nx, ny, nz, nch, nr, nvsm, readings, penalty;
+    int last_slice[2];  // last slice of each parity
     uint64_t n_items, nvsm1;
     float lambda, delta;
     double relax;  // step scale applied to the exact 1-D update before the positivity clamp
@@ -81,6 +87,70 @@ __device__ __forceinline__ float ldw<float>(const float* w, int64_t m) {
 template <>
 __device__ __forceinline__ float ldw<__half>(const __half* w, int64_t m) {
     return __half2float(__ldg(w + m));
+}
+
+// Entries m, m+32, ..., m+32(U-1) of a column: sinogram index (q + off, or
+// -1 past the end) and weight (0 past the end).
+template <int U, class WT>
+__device__ __forceinline__ void load_chunk(const int32_t* __restrict__ idx, const WT* __restrict__ w, int64_t m,
+                                           int64_t en, int off, int* q, float* wt) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int64_t mu = m + 32 * u;
+        if (mu < en) {
+            q[u] = __ldg(idx + mu) + off;
+            wt[u] = ldw(w, mu);
+        } else {
+            q[u] = -1;
+            wt[u] = 0.f;
+        }
+    }
+}
+
+constexpr int kU = 8;      // entries per lane in flight per chunk
+constexpr int kStack = 16;  // same-parity slices that sweep the sinogram together
+
+// Gather beta += a e and alpha += a^2 over entries [b, en) of a column: chunks
+// of 32 x kU entries, the next chunk's indices and weights fetched while this
+// chunk's e gathers are in flight (one DRAM round trip per chunk).
+template <class WT>
+__device__ __forceinline__ void gather_range(const int32_t* __restrict__ idx, const WT* __restrict__ w,
+                                             const float* e, int64_t b, int64_t en, int off, int lane,
+                                             float& acc_b, float& acc_a) {
+    if (b >= en) return;
+    int qa[kU];
+    float wa[kU];
+    load_chunk<kU>(idx, w, b + lane, en, off, qa, wa);
+    for (int64_t base = b; base < en; base += 32 * kU) {
+        float ev[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) ev[u] = (qa[u] >= 0) ? __ldcg(e + qa[u]) : 0.f;
+        int qb[kU];
+        float wb[kU];
+        load_chunk<kU>(idx, w, base + 32 * kU + lane, en, off, qb, wb);
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+            acc_b = fmaf(wa[u], ev[u], acc_b);
+            acc_a = fmaf(wa[u], wa[u], acc_a);
+            qa[u] = qb[u];
+            wa[u] = wb[u];
+        }
+    }
+}
+
+// e -= du * a over entries [b, en): kU independent index/weight loads per
+// lane per chunk, then kU fire-and-forget L2 reductions.
+template <class WT>
+__device__ __forceinline__ void scatter_range(const int32_t* __restrict__ idx, const WT* __restrict__ w, float* e,
+                                              int64_t b, int64_t en, int off, int lane, float du) {
+    for (int64_t base = b; base < en; base += 32 * kU) {
+        int qs[kU];
+        float ws[kU];
+        load_chunk<kU>(idx, w, base + lane, en, off, qs, ws);
+#pragma unroll
+        for (int u = 0; u < kU; ++u)
+            if (qs[u] >= 0) atomicAdd(e + qs[u], -du * ws[u]);
+    }
 }
 
 template <class WT>
@@ -116,39 +186,27 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
         const int64_t q = (int64_t)col + (int64_t)ncol * k;
         const int s = start[k];
         const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
-        int64_t b = 0, en = 0;
+        int64_t b = 0, en = 0, mid = 0;
         if (v1 > v0) {
             const int64_t cb = colptr[col];
-            b = cb + vptr[col * P.nvsm1 + v0];
-            en = cb + vptr[col * P.nvsm1 + v1];
+            const uint32_t* vp = vptr + col * P.nvsm1;
+            b = cb + vp[v0];
+            en = cb + vp[v1];
+            // Members of a slice stack (up to 16 same-parity slices at this
+            // physical position) all start their sweep at the data view where
+            // the stack's last member's window begins, then wrap around, so
+            // they read and update each sinogram sector at about the same time.
+            const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), P.last_slice[k % 2]);
+            const int vs = min(max(start[kl] - s, v0), v1);
+            mid = cb + vp[vs];
         }
         const int off = s * P.nch * P.nr;
 
-        // beta = sum a e, alpha = sum a^2 (FP32 accumulation per lane).
+        // beta = sum a e, alpha = sum a^2 (FP32 accumulation per lane) over
+        // [mid, en) then [b, mid).
         float acc_b = 0.f, acc_a = 0.f;
-        int64_t m = b + lane;
-        constexpr int U = 8;
-        for (; m + 32 * (U - 1) < en; m += 32 * U) {
-            int qi[U];
-            float wi[U], ev[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                qi[u] = __ldg(idx + m + 32 * u) + off;
-                wi[u] = ldw(w, m + 32 * u);
-            }
-#pragma unroll
-            for (int u = 0; u < U; ++u) ev[u] = __ldcg(e + qi[u]);
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                acc_b = fmaf(wi[u], ev[u], acc_b);
-                acc_a = fmaf(wi[u], wi[u], acc_a);
-            }
-        }
-        for (; m < en; m += 32) {
-            const float wv = ldw(w, m);
-            acc_b = fmaf(wv, __ldcg(e + __ldg(idx + m) + off), acc_b);
-            acc_a = fmaf(wv, wv, acc_a);
-        }
+        gather_range(idx, w, e, mid, en, off, lane, acc_b, acc_a);
+        gather_range(idx, w, e, b, mid, off, lane, acc_b, acc_a);
         const double beta = (double)warp_sum(acc_b);
         const double alpha = (double)warp_sum(acc_a);
 
@@ -207,17 +265,20 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
         if (lane == 0) x[q] = (float)(xq + upd);
         const float du = (float)upd;
         if (du != 0.f) {
-            for (int64_t mm = b + lane; mm < en; mm += 32)
-                atomicAdd(e + (__ldg(idx + mm) + off), -du * ldw(w, mm));
+            scatter_range(idx, w, e, mid, en, off, lane, du);
+            scatter_range(idx, w, e, b, mid, off, lane, du);
         }
     }
 }
 
 // Sort keys of the visiting order (see the file comment); voxels outside the
 // scanner FOV (icd_iteration.cpp:181) get the largest key and are dropped.
+//   key = ((cell-in-tile rank * Q + slice parity) * n_tiles + tile) * nz + slice
+// Tiles are T x T cells of the fixed frame; inside a tile cells follow a
+// serpentine raster, so consecutive stacks of a tile are neighbours.
 struct OrderParams {
-    int nx, ny, nz, P, Q, margin, lx, stride, gstride;
-    uint64_t lt;
+    int nx, ny, nz, T, Q, margin, lx;
+    uint64_t n_tiles;
     double cvx, cvy, vx, vy, fov_limit;
 };
 
@@ -239,11 +300,10 @@ __global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, 
         const double px = c * (i - O.cvx) - s * (j - O.cvy) + O.cvx;
         const double py = s * (i - O.cvx) + c * (j - O.cvy) + O.cvy;
         const int a = (int)llrint(px) + O.margin, b = (int)llrint(py) + O.margin;
-        const int off = (a % O.P) + O.P * (b % O.P);
-        const uint64_t rank_o = ((uint64_t)off * O.stride) % (uint64_t)(O.P * O.P);
-        const uint64_t cell = (uint64_t)(a / O.P) + (uint64_t)O.lx * (uint64_t)(b / O.P);
-        const uint64_t rank_c = (cell * O.gstride) % O.lt;
-        keys[t] = ((rank_o * O.Q + (uint64_t)(k % O.Q)) * O.lt + rank_c) * (uint64_t)O.nz + (uint64_t)k;
+        const int u = a % O.T, v = b % O.T;
+        const uint64_t rank_in_tile = (uint64_t)v * O.T + (uint64_t)((v & 1) ? (O.T - 1 - u) : u);
+        const uint64_t tile = (uint64_t)(a / O.T) + (uint64_t)O.lx * (uint64_t)(b / O.T);
+        keys[t] = ((rank_in_tile * O.Q + (uint64_t)(k % O.Q)) * O.n_tiles + tile) * (uint64_t)O.nz + (uint64_t)k;
     }
 }
 
@@ -272,21 +332,6 @@ __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uin
     }
 }
 
-int gcd(int a, int b) {
-    while (b) {
-        const int t = a % b;
-        a = b;
-        b = t;
-    }
-    return a;
-}
-
-int coprime_near(int target, int n) {
-    int s = std::max(1, target);
-    while (n > 1 && gcd(s, n) != 1) ++s;
-    return s;
-}
-
 GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o) {
     const ctbb_geom_c& g = rc->geom;
     GParams P;
@@ -299,6 +344,8 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     P.nvsm1 = ssm->nvsm + 1;
     P.readings = (int)g.Readings;
     P.penalty = g.penalty;
+    P.last_slice[(P.nz - 1) % 2] = P.nz - 1;
+    P.last_slice[P.nz % 2] = P.nz >= 2 ? P.nz - 2 : P.nz - 1;
     P.n_items = rc->n_order;
     P.lambda = (float)g.lambda;
     P.delta = (float)g.delta;
@@ -311,9 +358,12 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     return P;
 }
 
+// Tile edge T (cells): 8 tiles per axis by default (longer raster sweeps
+// converge faster per iteration, measured on the 512 x 512 x 64 workload);
+// `lattice` overrides it.
 int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     const int nx = (int)rc->geom.num_voxels_x;
-    int P = o.lattice > 0 ? o.lattice : (nx >= 256 ? 16 : (nx >= 64 ? 8 : 4));
+    const int P = o.lattice > 0 ? o.lattice : std::max(4, nx / 8);
     return std::max(1, std::min(P, nx));
 }
 
@@ -338,14 +388,13 @@ ctbb_status build_order(ctbb_recon* rc, int P_lat) {
     O.nx = (int)g.num_voxels_x;
     O.ny = (int)g.num_voxels_y;
     O.nz = (int)g.num_voxels_z;
-    O.P = P_lat;
+    O.T = P_lat;
     O.Q = O.nz >= 2 ? 2 : 1;
-    O.margin = P_lat * ((std::max(O.nx, O.ny) + P_lat - 1) / P_lat);
+    // Rotated voxel centres stay within (sqrt(2) - 1)/2 of the extent outside it.
+    O.margin = P_lat * ((std::max(O.nx, O.ny) / 4 + P_lat) / P_lat);
     O.lx = (O.nx + 2 * O.margin + P_lat - 1) / P_lat;
     const int ly = (O.ny + 2 * O.margin + P_lat - 1) / P_lat;
-    O.lt = (uint64_t)O.lx * ly;
-    O.stride = coprime_near(P_lat * P_lat / 2 + 1, P_lat * P_lat);
-    O.gstride = coprime_near((int)(0.6180339887 * (double)O.lt), (int)O.lt);
+    O.n_tiles = (uint64_t)O.lx * ly;
     O.cvx = g.center_voxel_x;
     O.cvy = g.center_voxel_y;
     O.vx = g.voxel_size_x;
@@ -441,13 +490,13 @@ ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out) {
 }
 
 int default_warps_in_flight(const ctbb_recon* rc) {
-    // Keep (voxels crossed per ray) * W / N near 0.4; a ray crosses about
-    // 4 * 0.8 * nx voxels (2 in-plane bilinear taps x 2 slices per x step).
+    // Keep (voxels crossed per ray) * W / N near 0.4 (a ray crosses about
+    // 4 * 0.8 * nx voxels: 2 in-plane bilinear taps x 2 slices per x step),
+    // W = warps = voxel updates in flight.
     const double n = (double)rc->nvox;
     const double per_ray = 3.2 * (double)rc->geom.num_voxels_x;
-    int w = (int)(0.4 * n / per_ray);
-    const int lo = 4, hi = rc->ctx->sm_count * 32;
-    return std::max(lo, std::min(hi, w));
+    const int w = (int)(0.4 * n / per_ray);
+    return std::max(4, std::min(rc->ctx->sm_count * 32, w));
 }
 
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
