@@ -190,16 +190,12 @@ def run_ours(args, rank, world, dist):
     if args.e2e:
         e2e = run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, torch, torch_stream)
 
-    t_max = elapsed_ms
-    if dist:
-        t = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_max = float(t.item())
-        if e2e:
-            te = torch.tensor([e2e["seconds"]], dtype=torch.float64, device="cuda")
-            dist.all_reduce(te, op=dist.ReduceOp.MAX)
-            e2e["seconds"] = float(te.item())
-            e2e["value"] = world * e2e["updates"] / e2e["seconds"]
+    from ctbb_icd_b200.replicas import max_over_ranks
+
+    t_max = max_over_ranks(elapsed_ms, dist, device="cuda")
+    if e2e and dist:
+        e2e["seconds"] = max_over_ranks(e2e["seconds"], dist, device="cuda")
+        e2e["value"] = world * e2e["updates"] / e2e["seconds"]
     out = None
     if rank == 0:
         peak, peak_kind = measured_peak()
