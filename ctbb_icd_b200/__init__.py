@@ -333,6 +333,36 @@ class Recon:
             pass
 
 
+class Batch:
+    """Independent reconstructions advanced together by one persistent launch
+    per iteration (ctbb_gpu_batch_*), replayed from a CUDA graph."""
+
+    def __init__(self, recons: list, ssms: list, ctx: Context | None = None):
+        self.ctx = ctx or recons[0].ctx
+        self.recons, self.ssms = list(recons), list(ssms)
+        rs = (C.c_void_p * len(recons))(*[r.handle.value for r in recons])
+        ss = (C.c_void_p * len(ssms))(*[s.handle.value for s in ssms])
+        h = C.c_void_p()
+        check(lib().ctbb_gpu_batch_create(self.ctx.handle, len(recons), rs, ss, C.byref(h)))
+        self.handle = h
+
+    def iterate(self, n_iter: int, opts: IcdOpts | None = None) -> IterStats:
+        st = IterStats()
+        check(lib().ctbb_gpu_batch_iterate(self.handle, C.byref(opts or icd_opts()), int(n_iter), C.byref(st)))
+        return st
+
+    def free(self):
+        if self.handle:
+            lib().ctbb_gpu_batch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
 # --------------------------------------------------------------------------
 # Stage functions with the reference's names
 # --------------------------------------------------------------------------

@@ -149,6 +149,9 @@ PROTOTYPES = {
     "ctbb_gpu_recon_entries": (_I, [_P, _P, _PD]),
     "ctbb_gpu_recon_refresh_residual": (_I, [_P, _P]),
     "ctbb_gpu_recon_cost": (_I, [_P, _PD]),
+    "ctbb_gpu_batch_create": (_I, [_P, _I, C.POINTER(_P), C.POINTER(_P), C.POINTER(_P)]),
+    "ctbb_gpu_batch_iterate": (_I, [_P, C.POINTER(IcdOpts), _I, C.POINTER(IterStats)]),
+    "ctbb_gpu_batch_free": (None, [_P]),
     "ctbb_gpu_icd": (_I, [_P, _P, _PG, _PU, _PF, _PF, C.POINTER(IcdOpts), C.POINTER(IterStats)]),
     "ctbb_gpu_rotate": (_I, [_P, _PG, _PD, _PU, _PF, _I]),
     "ctbb_gpu_rotate_device": (_I, [_P, _PG, _PD, _PU, _P, _P, _I]),

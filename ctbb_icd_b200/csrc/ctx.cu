@@ -58,8 +58,9 @@ extern "C" ctbb_status ctbb_gpu_init(int device, void* stream, ctbb_ctx** out) {
     return CTBB_OK;
 }
 
-extern "C" void ctbb_gpu_destroy(ctbb_ctx* ctx) {
-    if (!ctx) return;
+namespace {
+
+void teardown(ctbb_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     cudaFree(ctx->d_partials);
@@ -67,6 +68,31 @@ extern "C" void ctbb_gpu_destroy(ctbb_ctx* ctx) {
     cudaFree(ctx->d_flags);
     if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
+}
+
+}  // namespace
+
+namespace ctbb {
+
+void ctx_retain(ctbb_ctx* ctx) {
+    if (ctx) ctx->refs.fetch_add(1);
+}
+
+void ctx_release(ctbb_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->refs.fetch_sub(1) == 1 && ctx->closing.load()) teardown(ctx);
+}
+
+}  // namespace ctbb
+
+// Destroying a context that still has live matrices, reconstructions or
+// batches only marks it; the last of them to be freed tears it down, so the
+// order in which a caller (or a garbage collector) releases objects does not
+// matter.
+extern "C" void ctbb_gpu_destroy(ctbb_ctx* ctx) {
+    if (!ctx) return;
+    if (ctx->closing.exchange(true)) return;
+    if (ctx->refs.load() == 0) teardown(ctx);
 }
 
 extern "C" void* ctbb_gpu_stream(ctbb_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }

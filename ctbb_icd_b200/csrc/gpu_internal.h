@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <vector>
 
 #include "common.h"
@@ -26,6 +27,10 @@
     } while (0)
 
 struct ctbb_ctx {
+    // Objects (matrices, reconstructions, batches) created on this context;
+    // ctbb_gpu_destroy defers the teardown until the last of them is freed.
+    std::atomic<int> refs{0};
+    std::atomic<bool> closing{false};
     int device = 0;
     cudaStream_t stream = nullptr;
     bool own_stream = false;
@@ -84,6 +89,10 @@ struct ctbb_recon {
 };
 
 namespace ctbb {
+
+// Reference counting of a context by the objects created on it.
+void ctx_retain(ctbb_ctx* ctx);
+void ctx_release(ctbb_ctx* ctx);
 
 ctbb_status ensure_partials(ctbb_ctx* ctx, size_t n);
 

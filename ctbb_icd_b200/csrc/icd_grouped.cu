@@ -47,8 +47,11 @@
 // ray change concurrently; the default keeps that near 0.4.
 #include <math.h>
 
+#include <string.h>
+
 #include <algorithm>
 #include <cub/cub.cuh>
+#include <type_traits>
 #include <vector>
 
 #include "gpu_internal.h"
@@ -153,6 +156,125 @@ __device__ __forceinline__ void scatter_range(const int32_t* __restrict__ idx, c
     }
 }
 
+// Device-side view of one scan for the batched kernel.
+template <class WT>
+struct ScanRefs {
+    GParams P;
+    const uint32_t* order;
+    const int64_t* colptr;
+    const uint32_t* vptr;
+    const int32_t* idx;
+    const WT* w;
+    const int32_t* start;
+    float* e;
+    float* x;
+};
+
+// Penalised 1-D update of voxel q by one warp (lanes 0-7 hold the 8 in-plane
+// neighbours of penalties.cpp:41-52 / 67-74). Returns the step before the
+// positivity clamp; every lane gets the same value.
+__device__ __forceinline__ double penalty_step(const GParams& P, const float* x, int64_t q, double xq, double alpha,
+                                               double beta, int lane) {
+    const double r2 = 1.0 / 1.41421356237309504880168872420969807;
+    const int64_t nx = P.nx;
+    const int64_t nvox = (int64_t)P.nx * P.ny * P.nz;
+    double diff = 0.0, wn = 0.0;
+    if (lane < 8) {
+        const int64_t offs[8] = {-nx - 1, -nx, -nx + 1, -1, 1, nx - 1, nx, nx + 1};
+        const int64_t n = q + offs[lane];
+        if (n >= 0 && n < nvox) {
+            diff = (double)__ldcg(x + n) - xq;
+            wn = (lane == 1 || lane == 3 || lane == 4 || lane == 6) ? 1.0 : r2;
+        }
+    }
+    if (P.penalty == CTBB_PENALTY_QUADRATIC) {
+        // penalties.cpp:84 (the denominator always uses all 8 weights)
+        const double sum = sum8(wn * diff);
+        return (beta + (double)P.lambda * sum) / (alpha + (double)P.lambda * (4.0 + 4.0 * r2));
+    }
+    if (alpha == 0.0) return 0.0;  // penalties.cpp:101-102
+    // Root of f(d) = 2 alpha d - 2 beta + lambda sum w psi(d - diff),
+    // psi(t) = t / (delta + |t|), inside the reference's bracket.
+    const double lam = (double)P.lambda, del = (double)P.delta;
+    double lo = beta / alpha, hi = beta / alpha;
+    {
+        double dmin = (wn != 0.0) ? diff : lo, dmax = (wn != 0.0) ? diff : hi;
+#pragma unroll
+        for (int o2 = 1; o2 < 8; o2 <<= 1) {
+            dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o2));
+            dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o2));
+        }
+        lo = fmin(lo, __shfl_sync(0xffffffffu, dmin, 0));
+        hi = fmax(hi, __shfl_sync(0xffffffffu, dmax, 0));
+    }
+    double c = beta / alpha;
+    for (int it = 0; it < 64; ++it) {
+        const double t = c - diff;
+        const double den = del + fabs(t);
+        const double f = 2.0 * alpha * c - 2.0 * beta + lam * sum8(wn * t / den);
+        const double fp = 2.0 * alpha + lam * sum8(wn * del / (den * den));
+        if (f > 0.0)
+            hi = c;
+        else
+            lo = c;
+        double cn = c - f / fp;
+        if (!(cn > lo && cn < hi)) cn = 0.5 * (lo + hi);
+        const bool done = fabs(cn - c) <= 1e-12 * (1e-3 + fabs(c)) || (hi - lo) <= 1e-14;
+        c = cn;
+        if (done) break;
+    }
+    return c;
+}
+
+// One voxel update (work item `item` of a scan's visiting order) by one warp.
+template <class WT>
+__device__ __forceinline__ void process_item(const GParams& P, const uint32_t* __restrict__ order,
+                                             const int64_t* __restrict__ colptr, const uint32_t* __restrict__ vptr,
+                                             const int32_t* __restrict__ idx, const WT* __restrict__ w,
+                                             const int32_t* __restrict__ start, float* e, float* x, uint64_t item,
+                                             int lane) {
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint32_t packed = __ldg(order + item);
+    const uint64_t col = packed / (uint32_t)P.nz;
+    const int k = (int)(packed % (uint32_t)P.nz);
+    const int64_t q = (int64_t)col + (int64_t)ncol * k;
+    const int s = start[k];
+    const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+    int64_t b = 0, en = 0, mid = 0;
+    if (v1 > v0) {
+        const int64_t cb = colptr[col];
+        const uint32_t* vp = vptr + col * P.nvsm1;
+        b = cb + vp[v0];
+        en = cb + vp[v1];
+        // Members of a slice stack (up to 16 same-parity slices at this
+        // physical position) all start their sweep at the data view where the
+        // stack's last member's window begins, then wrap around, so they read
+        // and update each sinogram sector at about the same time.
+        const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), P.last_slice[k % 2]);
+        const int vs = min(max(start[kl] - s, v0), v1);
+        mid = cb + vp[vs];
+    }
+    const int off = s * P.nch * P.nr;
+
+    // beta = sum a e, alpha = sum a^2 (FP32 accumulation per lane) over
+    // [mid, en) then [b, mid).
+    float acc_b = 0.f, acc_a = 0.f;
+    gather_range(idx, w, e, mid, en, off, lane, acc_b, acc_a);
+    gather_range(idx, w, e, b, mid, off, lane, acc_b, acc_a);
+    const double beta = (double)warp_sum(acc_b);
+    const double alpha = (double)warp_sum(acc_a);
+
+    const double xq = (double)__ldcg(x + q);
+    double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+    if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+    if (lane == 0) x[q] = (float)(xq + upd);
+    const float du = (float)upd;
+    if (du != 0.f) {
+        scatter_range(idx, w, e, mid, en, off, lane, du);
+        scatter_range(idx, w, e, b, mid, off, lane, du);
+    }
+}
+
 template <class WT>
 __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint32_t* __restrict__ order,
                                                           const int64_t* __restrict__ colptr,
@@ -161,113 +283,42 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
                                                           const WT* __restrict__ w, const int32_t* __restrict__ start,
                                                           float* e, float* x, unsigned long long* queue) {
     const int lane = threadIdx.x & 31;
-    const double r2 = 1.0 / 1.41421356237309504880168872420969807;
-    // Neighbour offsets and weights of penalties.cpp:41-52 / 67-74 (lanes 0..7).
-    const int64_t nx = P.nx;
-    int64_t noff = 0;
-    double nw = 0.0;
-    if (lane < 8) {
-        const int64_t offs[8] = {-nx - 1, -nx, -nx + 1, -1, 1, nx - 1, nx, nx + 1};
-        noff = offs[lane];
-        nw = (lane == 1 || lane == 3 || lane == 4 || lane == 6) ? 1.0 : r2;
-    }
-    const double ws = 4.0 + 4.0 * r2;  // all 8 weights (the quadratic denominator always uses them)
-    const int64_t nvox = (int64_t)P.nx * P.ny * P.nz;
-    const uint64_t ncol = (uint64_t)P.nx * P.ny;
-
     for (;;) {
         unsigned long long item = 0;
         if (lane == 0) item = atomicAdd(queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= P.n_items) break;
-        const uint32_t packed = __ldg(order + item);
-        const uint64_t col = packed / (uint32_t)P.nz;
-        const int k = (int)(packed % (uint32_t)P.nz);
-        const int64_t q = (int64_t)col + (int64_t)ncol * k;
-        const int s = start[k];
-        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
-        int64_t b = 0, en = 0, mid = 0;
-        if (v1 > v0) {
-            const int64_t cb = colptr[col];
-            const uint32_t* vp = vptr + col * P.nvsm1;
-            b = cb + vp[v0];
-            en = cb + vp[v1];
-            // Members of a slice stack (up to 16 same-parity slices at this
-            // physical position) all start their sweep at the data view where
-            // the stack's last member's window begins, then wrap around, so
-            // they read and update each sinogram sector at about the same time.
-            const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), P.last_slice[k % 2]);
-            const int vs = min(max(start[kl] - s, v0), v1);
-            mid = cb + vp[vs];
-        }
-        const int off = s * P.nch * P.nr;
+        process_item(P, order, colptr, vptr, idx, w, start, e, x, item, lane);
+    }
+}
 
-        // beta = sum a e, alpha = sum a^2 (FP32 accumulation per lane) over
-        // [mid, en) then [b, mid).
-        float acc_b = 0.f, acc_a = 0.f;
-        gather_range(idx, w, e, mid, en, off, lane, acc_b, acc_a);
-        gather_range(idx, w, e, b, mid, off, lane, acc_b, acc_a);
-        const double beta = (double)warp_sum(acc_b);
-        const double alpha = (double)warp_sum(acc_a);
+// Batched variant: one persistent launch drains the merged queue of several
+// independent scans (`merged[t]` = scan << 40 | item within that scan).
+template <class WT>
+__global__ void __launch_bounds__(256) icd_batch_kernel(const ScanRefs<WT>* __restrict__ scans,
+                                                        const uint64_t* __restrict__ merged, uint64_t n_total,
+                                                        double relax, unsigned long long* queue) {
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(queue, 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n_total) break;
+        const uint64_t m = __ldg(merged + t);
+        const ScanRefs<WT>& S = scans[m >> 40];
+        GParams P = S.P;
+        P.relax = relax;
+        process_item(P, S.order, S.colptr, S.vptr, S.idx, S.w, S.start, S.e, S.x, m & ((1ull << 40) - 1), lane);
+    }
+}
 
-        // Neighbour differences x_n - x_q (lanes 0..7; weight 0 when outside).
-        const double xq = (double)__ldcg(x + q);
-        double diff = 0.0, wn = 0.0;
-        if (lane < 8) {
-            const int64_t n = q + noff;
-            if (n >= 0 && n < nvox) {
-                diff = (double)__ldcg(x + n) - xq;
-                wn = nw;
-            }
-        }
-        double upd;
-        if (P.penalty == CTBB_PENALTY_QUADRATIC) {
-            // penalties.cpp:84
-            const double sum = sum8(wn * diff);
-            upd = (beta + (double)P.lambda * sum) / (alpha + (double)P.lambda * ws);
-        } else if (alpha == 0.0) {
-            upd = 0.0;  // penalties.cpp:101-102
-        } else {
-            // Root of f(d) = 2 alpha d - 2 beta + lambda sum w psi(d - diff),
-            // psi(t) = t / (delta + |t|), inside the reference's bracket.
-            const double lam = (double)P.lambda, del = (double)P.delta;
-            double lo = beta / alpha, hi = beta / alpha;
-            {
-                double dmin = (wn != 0.0) ? diff : lo, dmax = (wn != 0.0) ? diff : hi;
-#pragma unroll
-                for (int o2 = 1; o2 < 8; o2 <<= 1) {
-                    dmin = fmin(dmin, __shfl_xor_sync(0xffffffffu, dmin, o2));
-                    dmax = fmax(dmax, __shfl_xor_sync(0xffffffffu, dmax, o2));
-                }
-                lo = fmin(lo, __shfl_sync(0xffffffffu, dmin, 0));
-                hi = fmax(hi, __shfl_sync(0xffffffffu, dmax, 0));
-            }
-            double c = beta / alpha;
-            for (int it = 0; it < 64; ++it) {
-                const double t = c - diff;
-                const double den = del + fabs(t);
-                const double f = 2.0 * alpha * c - 2.0 * beta + lam * sum8(wn * t / den);
-                const double fp = 2.0 * alpha + lam * sum8(wn * del / (den * den));
-                if (f > 0.0)
-                    hi = c;
-                else
-                    lo = c;
-                double cn = c - f / fp;
-                if (!(cn > lo && cn < hi)) cn = 0.5 * (lo + hi);
-                const bool done = fabs(cn - c) <= 1e-12 * (1e-3 + fabs(c)) || (hi - lo) <= 1e-14;
-                c = cn;
-                if (done) break;
-            }
-            upd = c;
-        }
-        upd *= P.relax;
-        if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
-        if (lane == 0) x[q] = (float)(xq + upd);
-        const float du = (float)upd;
-        if (du != 0.f) {
-            scatter_range(idx, w, e, mid, en, off, lane, du);
-            scatter_range(idx, w, e, b, mid, off, lane, du);
-        }
+// Merge keys: scan s's j-th item at fractional position (j + 0.5) / n_s, so
+// every scan has a share of the items in flight proportional to its size.
+__global__ void merge_keys_kernel(uint64_t n_s, uint32_t scan, uint64_t base, uint64_t* __restrict__ keys,
+                                  uint64_t* __restrict__ vals) {
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < n_s; j += (uint64_t)gridDim.x * blockDim.x) {
+        keys[base + j] = (uint64_t)(((double)j + 0.5) / (double)n_s * 4294967296.0) * 64ull + scan;
+        vals[base + j] = ((uint64_t)scan << 40) | j;
     }
 }
 
@@ -532,3 +583,229 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
 }
 
 }  // namespace ctbb
+
+// ---------------------------------------------------------------------------
+// Batched independent scans (one persistent launch per iteration for all of
+// them, replayed from a CUDA graph).
+// ---------------------------------------------------------------------------
+struct ctbb_batch {
+    ctbb_ctx* ctx = nullptr;
+    std::vector<ctbb_recon*> recons;
+    std::vector<const ctbb_ssm*> ssms;
+    uint64_t* d_merged = nullptr;
+    uint64_t n_total = 0;
+    std::vector<int> merged_T;  // tile edge per scan when d_merged was built
+    void* d_scans = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int graph_warps = 0, graph_weights = 0;
+    double graph_relax = 0.0;
+};
+
+namespace {
+
+using namespace ctbb;
+
+template <class WT>
+ctbb_status upload_scans(ctbb_batch* b, const ctbb_icd_opts& o) {
+    std::vector<ScanRefs<WT>> h(b->recons.size());
+    for (size_t i = 0; i < h.size(); ++i) {
+        ctbb_recon* rc = b->recons[i];
+        const ctbb_ssm* s = b->ssms[i];
+        h[i].P = make_params(rc, s, o);
+        h[i].order = rc->d_order;
+        h[i].colptr = s->d_colptr;
+        h[i].vptr = s->d_vptr;
+        h[i].idx = s->d_idx;
+        h[i].w = std::is_same<WT, __half>::value ? (const WT*)s->d_w16 : (const WT*)s->d_w32;
+        h[i].start = rc->d_start;
+        h[i].e = rc->d_e32;
+        h[i].x = rc->d_x32;
+    }
+    cudaFree(b->d_scans);
+    b->d_scans = nullptr;
+    CTBB_CUDA(cudaMalloc(&b->d_scans, h.size() * sizeof(ScanRefs<WT>)));
+    CTBB_CUDA(cudaMemcpyAsync(b->d_scans, h.data(), h.size() * sizeof(ScanRefs<WT>), cudaMemcpyHostToDevice,
+                              b->ctx->stream));
+    return CTBB_OK;
+}
+
+ctbb_status build_merged(ctbb_batch* b) {
+    cudaStream_t st = b->ctx->stream;
+    uint64_t n = 0;
+    for (ctbb_recon* rc : b->recons) n += rc->n_order;
+    uint64_t *k0 = nullptr, *k1 = nullptr, *v0 = nullptr, *v1 = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cudaMalloc(&k0, std::max<uint64_t>(1, n) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&k1, std::max<uint64_t>(1, n) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&v0, std::max<uint64_t>(1, n) * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&v1, std::max<uint64_t>(1, n) * 8);
+    uint64_t base = 0;
+    for (size_t i = 0; e == cudaSuccess && i < b->recons.size(); ++i) {
+        const uint64_t ns = b->recons[i]->n_order;
+        if (ns) {
+            const int grid = (int)std::min<uint64_t>((ns + 255) / 256, (uint64_t)b->ctx->sm_count * 16);
+            merge_keys_kernel<<<grid, 256, 0, st>>>(ns, (uint32_t)i, base, k0, v0);
+            e = cudaGetLastError();
+        }
+        base += ns;
+    }
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, k0, k1, v0, v1, (int)n, 0, 64, st);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, tmp_bytes);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, k0, k1, v0, v1, (int)n, 0, 64, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(k0);
+    cudaFree(k1);
+    cudaFree(v0);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+        cudaFree(v1);
+        return fail(e == cudaErrorMemoryAllocation ? CTBB_ERR_OOM : CTBB_ERR_CUDA, "batch queue: %s",
+                    cudaGetErrorString(e));
+    }
+    cudaFree(b->d_merged);
+    b->d_merged = v1;
+    b->n_total = n;
+    return CTBB_OK;
+}
+
+void drop_graph(ctbb_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+template <class WT>
+ctbb_status capture_iteration(ctbb_batch* b, int warps, double relax) {
+    drop_graph(b);
+    cudaStream_t st = b->ctx->stream;
+    const int blocks = std::max(1, (warps + 7) / 8);
+    cudaGraph_t g = nullptr;
+    CTBB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    cudaMemsetAsync(b->ctx->d_queue, 0, sizeof(unsigned long long), st);
+    icd_batch_kernel<WT><<<blocks, 256, 0, st>>>((const ScanRefs<WT>*)b->d_scans, b->d_merged, b->n_total, relax,
+                                                 b->ctx->d_queue);
+    const cudaError_t le = cudaGetLastError();
+    const cudaError_t ce = cudaStreamEndCapture(st, &g);
+    if (le != cudaSuccess || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return fail(CTBB_ERR_CUDA, "batch graph capture: %s",
+                    cudaGetErrorString(le != cudaSuccess ? le : ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return fail(CTBB_ERR_CUDA, "batch graph instantiate: %s", cudaGetErrorString(ie));
+    return CTBB_OK;
+}
+
+}  // namespace
+
+using namespace ctbb;
+
+extern "C" ctbb_status ctbb_gpu_batch_create(ctbb_ctx* ctx, int32_t n, ctbb_recon* const* recons,
+                                             const ctbb_ssm* const* ssms, ctbb_batch** out) {
+    clear_error();
+    if (!ctx || !recons || !ssms || !out || n <= 0) return fail(CTBB_ERR_INVALID_ARG, "null argument or empty batch");
+    if (n > 64) return fail(CTBB_ERR_INVALID_ARG, "a batch holds at most 64 scans (got %d)", n);
+    for (int i = 0; i < n; ++i) {
+        const ctbb_recon* rc = recons[i];
+        const ctbb_ssm* s = ssms[i];
+        if (!rc || !s) return fail(CTBB_ERR_INVALID_ARG, "scan %d: null reconstruction or matrix", i);
+        if (rc->ctx != ctx || s->ctx != ctx) return fail(CTBB_ERR_INVALID_ARG, "scan %d belongs to another context", i);
+        if (rc->geom.num_voxels_x != s->geom.num_voxels_x || rc->geom.num_voxels_y != s->geom.num_voxels_y ||
+            rc->geom.n_channels != s->geom.n_channels || rc->geom.Nrows_projection != s->geom.Nrows_projection ||
+            rc->geom.num_views_for_system_matrix != s->geom.num_views_for_system_matrix)
+            return fail(CTBB_ERR_INVALID_ARG, "scan %d: matrix geometry does not match the reconstruction", i);
+        for (int j = 0; j < i; ++j)
+            if (recons[j] == rc) return fail(CTBB_ERR_INVALID_ARG, "scan %d appears twice", i);
+    }
+    ctbb_batch* b = new ctbb_batch();
+    b->ctx = ctx;
+    ctx_retain(ctx);
+    b->recons.assign(recons, recons + n);
+    b->ssms.assign(ssms, ssms + n);
+    *out = b;
+    return CTBB_OK;
+}
+
+extern "C" ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* b, const ctbb_icd_opts* opts, int32_t n_iter,
+                                              ctbb_iter_stats* stats) {
+    clear_error();
+    if (!b || !opts) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (n_iter < 0) return fail(CTBB_ERR_INVALID_ARG, "negative iteration count");
+    CTBB_CUDA(cudaSetDevice(b->ctx->device));
+    const ctbb_icd_opts& o = *opts;
+    const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
+    if (wsel != CTBB_SSM_FP16 && wsel != CTBB_SSM_FP32) return fail(CTBB_ERR_INVALID_ARG, "weights must be FP16 or FP32");
+    double entries = 0.0;
+    int nx_max = 1;
+    bool orders_changed = b->d_merged == nullptr || b->merged_T.size() != b->recons.size();
+    std::vector<int> T(b->recons.size());
+    for (size_t i = 0; i < b->recons.size(); ++i) {
+        ctbb_recon* rc = b->recons[i];
+        const ctbb_ssm* s = b->ssms[i];
+        if ((wsel == CTBB_SSM_FP16 && !s->d_w16) || (wsel == CTBB_SSM_FP32 && !s->d_w32))
+            return fail(CTBB_ERR_INVALID_ARG, "scan %zu: matrix does not hold the requested weights", i);
+        CTBB_TRY(recon_to_grouped(rc, s));
+        T[i] = lattice_spacing(rc, o);
+        CTBB_TRY(build_order(rc, T[i]));
+        double en = 0.0;
+        CTBB_TRY(inrange_entries(rc, s, &en));
+        entries += en;
+        nx_max = std::max(nx_max, (int)rc->geom.num_voxels_x);
+        if (!orders_changed && b->merged_T[i] != T[i]) orders_changed = true;
+    }
+    if (orders_changed) {
+        CTBB_TRY(build_merged(b));
+        b->merged_T = T;
+        drop_graph(b);
+    }
+    const double relax = (o.relax > 0.0 && o.relax < 2.0) ? o.relax : 1.0;
+    // Each scan gets a share of the in-flight items proportional to its size,
+    // so the per-scan coupling bound uses the whole batch's item count.
+    const int warps = o.warps_in_flight > 0
+                          ? o.warps_in_flight
+                          : std::max(4, std::min(b->ctx->sm_count * 32, (int)(0.4 * (double)b->n_total / (3.2 * nx_max))));
+    if (!b->graph || b->graph_warps != warps || b->graph_relax != relax || b->graph_weights != wsel) {
+        if (wsel == CTBB_SSM_FP16) {
+            CTBB_TRY(upload_scans<__half>(b, o));
+            CTBB_TRY(capture_iteration<__half>(b, warps, relax));
+        } else {
+            CTBB_TRY(upload_scans<float>(b, o));
+            CTBB_TRY(capture_iteration<float>(b, warps, relax));
+        }
+        b->graph_warps = warps;
+        b->graph_relax = relax;
+        b->graph_weights = wsel;
+    }
+    cudaStream_t st = b->ctx->stream;
+    cudaEvent_t e0, e1;
+    CTBB_CUDA(cudaEventCreate(&e0));
+    CTBB_CUDA(cudaEventCreate(&e1));
+    CTBB_CUDA(cudaEventRecord(e0, st));
+    for (int it = 0; it < n_iter; ++it) CTBB_CUDA(cudaGraphLaunch(b->graph, st));
+    CTBB_CUDA(cudaEventRecord(e1, st));
+    CTBB_CUDA(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (stats) {
+        memset(stats, 0, sizeof(*stats));
+        stats->iterations = n_iter;
+        stats->device_ms = ms;
+        stats->voxel_updates = (double)b->n_total * n_iter;
+        stats->entries = entries * n_iter;
+    }
+    return CTBB_OK;
+}
+
+extern "C" void ctbb_gpu_batch_free(ctbb_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    cudaStreamSynchronize(b->ctx->stream);
+    drop_graph(b);
+    cudaFree(b->d_merged);
+    cudaFree(b->d_scans);
+    ctx_release(b->ctx);
+    delete b;
+}

@@ -253,6 +253,7 @@ extern "C" ctbb_status ctbb_gpu_recon_create(ctbb_ctx* ctx, const ctbb_geom_c* g
         }
     } guard{rc};
     rc->ctx = ctx;
+    ctx_retain(ctx);
     rc->geom = *geom;
     rc->nvox = geom->num_voxels_x * geom->num_voxels_y * geom->num_voxels_z;
     rc->data_size = geom->Readings * geom->n_channels * geom->Nrows_projection;
@@ -294,6 +295,7 @@ extern "C" void ctbb_gpu_recon_free(ctbb_recon* rc) {
     cudaFree(rc->d_x64);
     cudaFree(rc->d_x32);
     cudaFree(rc->d_order);
+    ctx_release(rc->ctx);
     delete rc;
 }
 

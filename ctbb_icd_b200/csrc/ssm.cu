@@ -279,6 +279,7 @@ void free_ssm(ctbb_ssm* s) {
     cudaFree(s->d_idx);
     cudaFree(s->d_w32);
     cudaFree(s->d_w16);
+    ctbb::ctx_release(s->ctx);
     delete s;
 }
 
@@ -431,6 +432,7 @@ extern "C" ctbb_status ctbb_gpu_generate_ssm(ctbb_ctx* ctx, const ctbb_geom_c* g
 
     ctbb_ssm* s = new ctbb_ssm();
     s->ctx = ctx;
+    ctbb::ctx_retain(ctx);
     s->geom = g;
     s->ncol = (uint64_t)P.nx * P.ny;
     s->nvsm = (uint64_t)P.nvsm;
@@ -656,6 +658,7 @@ extern "C" ctbb_status ctbb_gpu_ssm_import_reference(ctbb_ctx* ctx, const ctbb_g
         }
     } guard{s};
     s->ctx = ctx;
+    ctbb::ctx_retain(ctx);
     s->geom = g;
     s->ncol = ncol;
     s->nvsm = nvsm;

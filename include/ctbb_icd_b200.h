@@ -314,6 +314,22 @@ ctbb_status ctbb_gpu_recon_refresh_residual(ctbb_recon* rc, const ctbb_ssm* ssm)
 ctbb_status ctbb_gpu_recon_cost(ctbb_recon* rc, double* cost);
 
 /*
+ * Several independent reconstructions advanced together (no reference
+ * counterpart: the reference reconstructs one scan per process). Each
+ * iteration is one persistent launch that drains the merged work queue of
+ * all scans, each scan's items spread in proportion to its size, replayed
+ * from a CUDA graph captured on the context's stream. Up to 64 scans of one
+ * context, each with its own matrix; opts->weights must be held by every
+ * matrix. The scans keep their own state (ctbb_gpu_recon_* still apply).
+ */
+typedef struct ctbb_batch ctbb_batch;
+ctbb_status ctbb_gpu_batch_create(ctbb_ctx* ctx, int32_t n, ctbb_recon* const* recons,
+                                  const ctbb_ssm* const* ssms, ctbb_batch** out);
+ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* batch, const ctbb_icd_opts* opts, int32_t n_iter,
+                                   ctbb_iter_stats* stats);
+void ctbb_gpu_batch_free(ctbb_batch* batch);
+
+/*
  * One-call drop-in for icd_iteration (src/icd_iteration.cpp:42-286): copies
  * raw and recon_volume (initial image) from the host, runs
  * geom->num_iterations iterations and writes the result back to recon_volume.

@@ -212,3 +212,38 @@ def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights):
     assert all(b <= a * (1 + 1e-9) for a, b in zip(costs, costs[1:])), costs
     assert rmse_hu <= 0.5, rmse_hu
     assert abs(costs[-1] - cost_ref) <= 1e-6 * abs(cost_ref), (costs[-1], cost_ref)
+
+
+def test_batch_of_uneven_scans_converges(ctx, converged_cfg1_small, tmp_path):
+    rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
+    scans = []
+    for name in ("small", "small_ffs"):
+        _, rpo = W.materialise(name, str(tmp_path / name))
+        d = C.load_raw(rpo)
+        s = C.Ssm.generate(rpo, ctx, C.SSM_BOTH)
+        r = C.Recon(rpo, d.slice_indices, ctx)
+        r.set_raw(d.raw)
+        r.set_volume(s, None)
+        scans.append((r, s, r.cost()))
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    batch = C.Batch([rc] + [r for r, _, _ in scans], [ssm] + [s for _, s, _ in scans], ctx)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
+    total = int(np.prod(rp.shape)) + sum(int(np.prod(r.rp.shape)) for r, _, _ in scans)
+    st = batch.iterate(15, opts)
+    assert st.iterations == 15 and st.voxel_updates == 15 * total and st.device_ms > 0
+    mid = []
+    for r, s, _ in scans:
+        r.refresh_residual(s)
+        mid.append(r.cost())
+    batch.iterate(15, opts)  # replays the captured iteration graph
+    rc.refresh_residual(ssm)
+    x = rc.volume_f64()
+    rmse_hu = np.sqrt(np.mean((x - x_ref) ** 2)) / HU
+    assert rmse_hu <= 0.5, rmse_hu
+    assert abs(rc.cost() - cost_ref) <= 1e-6 * abs(cost_ref)
+    for (r, s, c0), c15 in zip(scans, mid):
+        r.refresh_residual(s)
+        assert r.cost() < c15 < c0, (c0, c15, r.cost())
+    batch.free()
