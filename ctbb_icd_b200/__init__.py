@@ -33,7 +33,7 @@ __all__ = [
     "configure_recon_params", "load_raw", "initialize_recon_volume", "generate_system_matrix",
     "generate_system_matrix_ffs", "icd_iteration", "rotate_slices_rotating2fixed",
     "rotate_slices_fixed2rotating", "clean_up", "synth_raw_host", "write_raw_file",
-    "slice_tables", "icd_opts",
+    "slice_tables", "icd_opts", "WarmStartNet",
 ]
 
 
@@ -251,12 +251,13 @@ class Ssm:
 
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
-             compute_cost=False, stop_rel_change=0.0, relax=0.0) -> IcdOpts:
+             compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
     o.compute_cost, o.stop_rel_change = int(bool(compute_cost)), float(stop_rel_change)
     o.relax = float(relax)
+    o.priority = int(bool(priority))
     return o
 
 
@@ -320,6 +321,33 @@ class Recon:
         c = C.c_double()
         check(lib().ctbb_gpu_recon_cost(self.handle, C.byref(c)))
         return c.value
+
+    def autotune(self, ssm: Ssm, opts: IcdOpts | None = None, probe_iters: int = 2):
+        """Pick warps in flight and the visiting-order tile edge by measured
+        cost decrease per device second (ctbb_gpu_recon_autotune). Returns
+        (tuned opts, list of trial dicts); the iterate is left unchanged."""
+        from ._lib import TuneReport
+
+        best, rep = IcdOpts(), TuneReport()
+        check(lib().ctbb_gpu_recon_autotune(self.handle, ssm.handle, C.byref(opts or icd_opts()),
+                                            int(probe_iters), C.byref(best), C.byref(rep)))
+        trials = [dict(warps_in_flight=t.warps_in_flight, lattice=t.lattice, device_ms=t.device_ms,
+                       cost=t.cost, score=t.score, best=(i == rep.best))
+                  for i, t in enumerate(rep.trials[:rep.n_trials])]
+        return best, trials
+
+    def warm_start(self, ssm: Ssm, net, tube_angles: np.ndarray):
+        """Add the network's predicted correction to the current iterate
+        (fixed-frame prediction, rotated back), refresh e = y - Ax and keep the
+        per-voxel step as the priority map (ctbb_gpu_recon_warm_start)."""
+        ta = np.ascontiguousarray(tube_angles, dtype=np.float64)
+        check(lib().ctbb_gpu_recon_warm_start(self.handle, ssm.handle, net.handle, ptr(ta, C.c_double)))
+
+    def set_priority(self, fraction: float, opts: IcdOpts | None = None):
+        """Priority passes (icd_opts(priority=True)) visit the `fraction` of
+        voxels with the largest warm-start step."""
+        o = opts or icd_opts()
+        check(lib().ctbb_gpu_recon_set_priority(self.handle, C.byref(o), float(fraction)))
 
     def free(self):
         if self.handle:
@@ -423,3 +451,6 @@ def clean_up(rp: ReconParams, data: CtData) -> str:
         data.system_matrix.free()
         data.system_matrix = None
     return path
+
+
+from .learned import WarmStartNet  # noqa: E402

@@ -99,7 +99,16 @@ class IcdOpts(C.Structure):
     _fields_ = [
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
+        ("priority", _I), ("reserved2", _I),
     ]
+
+
+class TuneTrial(C.Structure):
+    _fields_ = [("warps_in_flight", _I), ("lattice", _I), ("device_ms", _D), ("cost", _D), ("score", _D)]
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("n_trials", _I), ("best", _I), ("start_cost", _D), ("trials", TuneTrial * 32)]
 
 
 class IterStats(C.Structure):
@@ -156,6 +165,21 @@ PROTOTYPES = {
     "ctbb_gpu_rotate": (_I, [_P, _PG, _PD, _PU, _PF, _I]),
     "ctbb_gpu_rotate_device": (_I, [_P, _PG, _PD, _PU, _P, _P, _I]),
     "ctbb_gpu_rotate_device_noalloc": (_I, [_P, _PG, _PD, _PU, _P, _P, _I]),
+    "ctbb_cnn_create": (_I, [_P, _I, _U, C.POINTER(_P)]),
+    "ctbb_cnn_free": (None, [_P]),
+    "ctbb_cnn_num_params": (_U, [_P]),
+    "ctbb_cnn_get_params": (_I, [_P, _PF, _U]),
+    "ctbb_cnn_set_params": (_I, [_P, _PF, _U]),
+    "ctbb_cnn_set_scaling": (_I, [_P, C.c_float, C.c_float]),
+    "ctbb_cnn_get_scaling": (_I, [_P, _PF, _PF]),
+    "ctbb_cnn_forward": (_I, [_P, _P, _I, _I, _I, _P]),
+    "ctbb_cnn_accumulate_gradient": (_I, [_P, _P, _P, _P, _I, _I, _I, _PD]),
+    "ctbb_cnn_get_gradient": (_I, [_P, _PF, _U]),
+    "ctbb_cnn_zero_gradient": (_I, [_P]),
+    "ctbb_cnn_adam_step": (_I, [_P, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "ctbb_gpu_recon_warm_start": (_I, [_P, _P, _P, _PD]),
+    "ctbb_gpu_recon_autotune": (_I, [_P, _P, C.POINTER(IcdOpts), _I, C.POINTER(IcdOpts), C.POINTER(TuneReport)]),
+    "ctbb_gpu_recon_set_priority": (_I, [_P, C.POINTER(IcdOpts), _D]),
 }
 
 _lib = None

@@ -86,7 +86,14 @@ struct ctbb_recon {
     uint32_t* d_order = nullptr;
     uint64_t n_order = 0;
     int order_P = 0;
+    // Learned warm start: per-voxel priority (size of the warm-start step)
+    // and the visiting order restricted to the highest-priority voxels.
+    float* d_prio = nullptr;
+    uint32_t* d_prio_order = nullptr;
+    uint64_t n_prio_order = 0;
 };
+
+struct ctbb_cnn;
 
 namespace ctbb {
 
@@ -110,8 +117,17 @@ ctbb_status launch_icd_sequential(ctbb_recon* rc, const ctbb_ssm* ssm, int n_ite
 
 // icd_grouped.cu
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o,
-                               float* ms, double* entries);
+                               float* ms, double* entries, uint64_t* items);
 int default_warps_in_flight(const ctbb_recon* rc);
 ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out);
+
+// rotate.cu
+ctbb_status rotate_volume(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tube_angles_deg,
+                          const uint64_t* slice_indices, const float* d_in, float* d_out, int direction);
+
+// cnn.cu
+ctbb_status cnn_predict_correction(ctbb_cnn* c, const float* x_dev, int nx, int ny, int nz, float* d_dev);
+ctbb_status apply_correction(ctbb_ctx* ctx, uint64_t n, float* x_dev, const float* d_dev, float* prio_dev);
+ctbb_ctx* cnn_ctx(const ctbb_cnn* c);
 
 }  // namespace ctbb

@@ -333,8 +333,8 @@ struct OrderParams {
     double cvx, cvy, vx, vy, fov_limit;
 };
 
-__global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, uint64_t* __restrict__ keys,
-                                  uint32_t* __restrict__ vals) {
+__global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, const float* __restrict__ prio,
+                                  float thr, uint64_t* __restrict__ keys, uint32_t* __restrict__ vals) {
     const uint64_t ncol = (uint64_t)O.nx * O.ny, n = ncol * O.nz;
     for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
         const int k = (int)(t / ncol);
@@ -342,7 +342,7 @@ __global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, 
         const int i = (int)(col % O.nx), j = (int)(col / O.nx);
         vals[t] = (uint32_t)(col * O.nz + k);
         const double xx = (i - O.cvx) * O.vx, yy = (j - O.cvy) * O.vy;
-        if (!(xx * xx + yy * yy < O.fov_limit)) {
+        if (!(xx * xx + yy * yy < O.fov_limit) || (prio && !(prio[t] >= thr))) {
             keys[t] = ~0ull;
             continue;
         }
@@ -418,10 +418,11 @@ int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     return std::max(1, std::min(P, nx));
 }
 
-// Build (or reuse) the visiting order for lattice spacing P_lat.
-ctbb_status build_order(ctbb_recon* rc, int P_lat) {
+// Visiting order for tile edge P_lat, optionally restricted to the voxels
+// whose priority is at least thr.
+ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float thr, uint32_t** out,
+                             uint64_t* n_out) {
     using namespace ctbb;
-    if (rc->d_order && rc->order_P == P_lat) return CTBB_OK;
     const ctbb_geom_c& g = rc->geom;
     ctbb_ctx* ctx = rc->ctx;
     cudaStream_t st = ctx->stream;
@@ -473,7 +474,7 @@ ctbb_status build_order(ctbb_recon* rc, int P_lat) {
     if (e == cudaSuccess) e = cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
         const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
-        order_keys_kernel<<<grid, 256, 0, st>>>(O, d_cs, d_k0, d_v0);
+        order_keys_kernel<<<grid, 256, 0, st>>>(O, d_cs, prio, thr, d_k0, d_v0);
         e = cudaGetLastError();
     }
     if (e == cudaSuccess)
@@ -509,11 +510,22 @@ ctbb_status build_order(ctbb_recon* rc, int P_lat) {
         cleanup();
         return rcode;
     }
-    cudaFree(rc->d_order);
-    rc->d_order = d_v1;
-    rc->n_order = n_valid;
-    rc->order_P = P_lat;
+    *out = d_v1;
+    *n_out = n_valid;
     cleanup();
+    return CTBB_OK;
+}
+
+// Build (or reuse) the full visiting order for tile edge P_lat.
+ctbb_status build_order(ctbb_recon* rc, int P_lat) {
+    if (rc->d_order && rc->order_P == P_lat) return CTBB_OK;
+    uint32_t* o = nullptr;
+    uint64_t n = 0;
+    CTBB_TRY(build_order_into(rc, P_lat, nullptr, 0.f, &o, &n));
+    cudaFree(rc->d_order);
+    rc->d_order = o;
+    rc->n_order = n;
+    rc->order_P = P_lat;
     return CTBB_OK;
 }
 
@@ -551,10 +563,20 @@ int default_warps_in_flight(const ctbb_recon* rc) {
 }
 
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
-                               double* entries) {
+                               double* entries, uint64_t* items) {
     CTBB_TRY(build_order(rc, lattice_spacing(rc, o)));
-    const GParams P = make_params(rc, ssm, o);
-    if (entries) CTBB_TRY(inrange_entries(rc, ssm, entries));
+    if (o.priority && !rc->d_prio_order)
+        return fail(CTBB_ERR_INVALID_ARG, "priority pass requested but no priority set (ctbb_gpu_recon_set_priority)");
+    const bool prio = o.priority != 0;
+    GParams P = make_params(rc, ssm, o);
+    if (prio) P.n_items = rc->n_prio_order;
+    const uint32_t* order = prio ? rc->d_prio_order : rc->d_order;
+    if (items) *items = P.n_items;
+    if (entries) {
+        CTBB_TRY(inrange_entries(rc, ssm, entries));
+        // A priority pass visits a subset; scale by the share of items.
+        if (prio && rc->n_order > 0) *entries *= (double)rc->n_prio_order / (double)rc->n_order;
+    }
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
     const int blocks = std::max(1, (W + 7) / 8);
     ctbb_ctx* ctx = rc->ctx;
@@ -566,11 +588,11 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     CTBB_CUDA(cudaEventRecord(e0, st));
     const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
     if (wsel == CTBB_SSM_FP16)
-        icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, rc->d_order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
+        icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
                                                            ssm->d_w16, rc->d_start, rc->d_e32, rc->d_x32,
                                                            ctx->d_queue);
     else
-        icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, rc->d_order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
+        icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
                                                           ssm->d_w32, rc->d_start, rc->d_e32, rc->d_x32,
                                                           ctx->d_queue);
     CTBB_CUDA(cudaGetLastError());
@@ -808,4 +830,43 @@ extern "C" void ctbb_gpu_batch_free(ctbb_batch* b) {
     cudaFree(b->d_scans);
     ctx_release(b->ctx);
     delete b;
+}
+
+// ---------------------------------------------------------------------------
+// Priority subset (voxels with the largest predicted change first).
+// ---------------------------------------------------------------------------
+extern "C" ctbb_status ctbb_gpu_recon_set_priority(ctbb_recon* rc, const ctbb_icd_opts* opts, double fraction) {
+    clear_error();
+    if (!rc) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (!rc->d_prio) return fail(CTBB_ERR_INVALID_ARG, "no priority map (run ctbb_gpu_recon_warm_start first)");
+    if (!(fraction > 0.0 && fraction <= 1.0)) return fail(CTBB_ERR_INVALID_ARG, "fraction must be in (0, 1]");
+    CTBB_CUDA(cudaSetDevice(rc->ctx->device));
+    ctbb_icd_opts o{};
+    if (opts) o = *opts;
+    cudaStream_t st = rc->ctx->stream;
+    const uint64_t n = rc->nvox;
+    // Threshold: the (1 - fraction) quantile of the priority map.
+    float* d_sorted = nullptr;
+    void* d_tmp = nullptr;
+    size_t tmp_bytes = 0;
+    float thr = 0.f;
+    cudaError_t e = cudaMalloc(&d_sorted, n * sizeof(float));
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(nullptr, tmp_bytes, rc->d_prio, d_sorted, (int)n, 0, 32, st);
+    if (e == cudaSuccess) e = cudaMalloc(&d_tmp, tmp_bytes);
+    if (e == cudaSuccess) e = cub::DeviceRadixSort::SortKeys(d_tmp, tmp_bytes, rc->d_prio, d_sorted, (int)n, 0, 32, st);
+    if (e == cudaSuccess) {
+        const uint64_t q = std::min<uint64_t>(n - 1, (uint64_t)((1.0 - fraction) * (double)n));
+        e = cudaMemcpyAsync(&thr, d_sorted + q, sizeof(float), cudaMemcpyDeviceToHost, st);
+    }
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(d_sorted);
+    cudaFree(d_tmp);
+    if (e != cudaSuccess) return fail(CTBB_ERR_CUDA, "priority threshold: %s", cudaGetErrorString(e));
+    uint32_t* order = nullptr;
+    uint64_t n_order = 0;
+    CTBB_TRY(build_order_into(rc, lattice_spacing(rc, o), rc->d_prio, thr, &order, &n_order));
+    cudaFree(rc->d_prio_order);
+    rc->d_prio_order = order;
+    rc->n_prio_order = n_order;
+    return CTBB_OK;
 }

@@ -295,6 +295,8 @@ extern "C" void ctbb_gpu_recon_free(ctbb_recon* rc) {
     cudaFree(rc->d_x64);
     cudaFree(rc->d_x32);
     cudaFree(rc->d_order);
+    cudaFree(rc->d_prio);
+    cudaFree(rc->d_prio_order);
     ctx_release(rc->ctx);
     delete rc;
 }
@@ -430,6 +432,7 @@ extern "C" ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ss
     for (int it = 0; it < n_iter; ++it) {
         float ms = 0.f;
         double entries = 0.0;
+        double upd = (double)rc->nvox;
         if (opts->mode == CTBB_ICD_SEQUENTIAL) {
             if (!ssm->d_w32) return fail(CTBB_ERR_INVALID_ARG, "sequential mode needs FP32 weights");
             CTBB_TRY(recon_to_sequential(rc, ssm));
@@ -445,14 +448,16 @@ extern "C" ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ss
                     rc->d_raw, rc->d_est64, rc->d_e32, rc->data_size);
                 CTBB_CUDA(cudaGetLastError());
             }
-            CTBB_TRY(launch_icd_grouped(rc, ssm, *opts, &ms, &entries));
+            uint64_t items = 0;
+            CTBB_TRY(launch_icd_grouped(rc, ssm, *opts, &ms, &entries, &items));
+            if (opts->priority) upd = (double)items;
         } else {
             return fail(CTBB_ERR_INVALID_ARG, "unknown ICD mode %d", opts->mode);
         }
         s.iterations += 1;
         s.device_ms += ms;
         s.entries += entries;
-        s.voxel_updates += (double)rc->nvox;
+        s.voxel_updates += upd;
         if (opts->compute_cost || opts->stop_rel_change > 0.0) {
             double c = 0.0;
             CTBB_TRY(cost_f64(rc, ssm, false, &c));
@@ -489,5 +494,41 @@ extern "C" ctbb_status ctbb_gpu_icd(ctbb_ctx* ctx, const ctbb_ssm* ssm, const ct
     if (st == CTBB_OK) st = ctbb_gpu_recon_iterate(rc, ssm, &o, (int32_t)geom->num_iterations, stats);
     if (st == CTBB_OK) st = ctbb_gpu_recon_get_volume(rc, recon_volume);
     ctbb_gpu_recon_free(rc);
+    return st;
+}
+
+// Learned warm start: x <- max(0, x + R_fixed2rot(cnn(R_rot2fixed(x)))), then
+// e = y - Ax in FP64; the per-voxel step size becomes the priority map.
+extern "C" ctbb_status ctbb_gpu_recon_warm_start(ctbb_recon* rc, const ctbb_ssm* ssm, ctbb_cnn* cnn,
+                                                 const double* tube_angles_deg) {
+    clear_error();
+    if (!rc || !ssm || !cnn || !tube_angles_deg) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    CTBB_TRY(check_pair(rc, ssm));
+    if (cnn_ctx(cnn) != rc->ctx) return fail(CTBB_ERR_INVALID_ARG, "network and reconstruction use different contexts");
+    CTBB_CUDA(cudaSetDevice(rc->ctx->device));
+    CTBB_TRY(recon_to_grouped(rc, ssm));
+    const ctbb_geom_c& g = rc->geom;
+    const uint64_t n = rc->nvox;
+    if (!rc->d_prio) CTBB_CUDA(cudaMalloc(&rc->d_prio, n * sizeof(float)));
+    float *d_a = nullptr, *d_b = nullptr;
+    CTBB_CUDA(cudaMalloc(&d_a, n * sizeof(float)));
+    if (cudaMalloc(&d_b, n * sizeof(float)) != cudaSuccess) {
+        cudaFree(d_a);
+        return fail(CTBB_ERR_OOM, "warm start scratch");
+    }
+    ctbb_status st = rotate_volume(rc->ctx, g, tube_angles_deg, rc->slice_indices.data(), rc->d_x32, d_a,
+                                   CTBB_ROTATE_ROTATING2FIXED);
+    if (st == CTBB_OK)
+        st = cnn_predict_correction(cnn, d_a, (int)g.num_voxels_x, (int)g.num_voxels_y, (int)g.num_voxels_z, d_b);
+    if (st == CTBB_OK)
+        st = rotate_volume(rc->ctx, g, tube_angles_deg, rc->slice_indices.data(), d_b, d_a,
+                           CTBB_ROTATE_FIXED2ROTATING);
+    if (st == CTBB_OK) st = apply_correction(rc->ctx, n, rc->d_x32, d_a, rc->d_prio);
+    if (st == CTBB_OK) st = ctbb_gpu_recon_refresh_residual(rc, ssm);
+    cudaFree(d_a);
+    cudaFree(d_b);
+    cudaFree(rc->d_prio_order);
+    rc->d_prio_order = nullptr;
+    rc->n_prio_order = 0;
     return st;
 }

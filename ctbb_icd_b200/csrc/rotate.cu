@@ -101,6 +101,13 @@ ctbb_status rotate_device(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tub
 
 using namespace ctbb;
 
+namespace ctbb {
+ctbb_status rotate_volume(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tube_angles_deg,
+                          const uint64_t* slice_indices, const float* d_in, float* d_out, int direction) {
+    return rotate_device(ctx, g, tube_angles_deg, slice_indices, d_in, d_out, direction);
+}
+}  // namespace ctbb
+
 extern "C" ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* geom, const double* tube_angles_deg,
                                               const uint64_t* slice_indices, const float* in_dev, float* out_dev,
                                               int32_t direction) {

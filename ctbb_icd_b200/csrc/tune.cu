@@ -1,0 +1,122 @@
+// Autotuner for grouped ICD (no reference counterpart; the reference has one
+// sequential order). Picks the number of concurrent voxel updates (warps in
+// flight) and the tile edge of the visiting order by the measured decrease
+// of the FP64 cost per millisecond of device time, probed from the current
+// iterate; the iterate and error sinogram are restored afterwards.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gpu_internal.h"
+
+using namespace ctbb;
+
+extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts* base,
+                                               int32_t probe_iters, ctbb_icd_opts* best, ctbb_tune_report* report) {
+    clear_error();
+    if (!rc || !ssm || !best) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (probe_iters <= 0 || probe_iters > 100) return fail(CTBB_ERR_INVALID_ARG, "probe_iters must be in [1, 100]");
+    ctbb_icd_opts o{};
+    if (base) o = *base;
+    o.mode = CTBB_ICD_GROUPED;
+    o.priority = 0;
+    const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
+    if ((wsel == CTBB_SSM_FP32 && !ssm->d_w32) || (wsel == CTBB_SSM_FP16 && !ssm->d_w16))
+        return fail(CTBB_ERR_INVALID_ARG, "requested weight format is not held by the matrix");
+    o.weights = wsel;
+    CTBB_CUDA(cudaSetDevice(rc->ctx->device));
+    CTBB_TRY(recon_to_grouped(rc, ssm));
+    CTBB_TRY(ctbb_gpu_recon_refresh_residual(rc, ssm));
+    double c0 = 0.0;
+    CTBB_TRY(cost_f64(rc, ssm, false, &c0));
+    cudaStream_t st = rc->ctx->stream;
+    float *d_xs = nullptr, *d_es = nullptr;
+    CTBB_CUDA(cudaMalloc(&d_xs, rc->nvox * sizeof(float)));
+    if (cudaMalloc(&d_es, rc->data_size * sizeof(float)) != cudaSuccess) {
+        cudaFree(d_xs);
+        return fail(CTBB_ERR_OOM, "autotune snapshot");
+    }
+    auto copy = [&](float* dst_x, const float* src_x, float* dst_e, const float* src_e) {
+        cudaError_t e = cudaMemcpyAsync(dst_x, src_x, rc->nvox * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dst_e, src_e, rc->data_size * sizeof(float), cudaMemcpyDeviceToDevice, st);
+        return e;
+    };
+    ctbb_status status = CTBB_OK;
+    if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
+
+    // Candidates: multiples of the coupling-bound default, and tile edges of
+    // 1/16, 1/8 and 1/4 of the slice.
+    const int w0 = default_warps_in_flight(rc);
+    const int wmax = rc->ctx->sm_count * 48;
+    std::vector<int> ws;
+    for (int m : {1, 2, 4, 8, 16, 32}) {
+        const int w = std::max(32, std::min(wmax, w0 * m));
+        if (std::find(ws.begin(), ws.end(), w) == ws.end()) ws.push_back(w);
+    }
+    const int nx = (int)rc->geom.num_voxels_x;
+    std::vector<int> ts;
+    for (int d : {16, 8, 4}) {
+        const int t = std::max(4, nx / d);
+        if (std::find(ts.begin(), ts.end(), t) == ts.end()) ts.push_back(t);
+    }
+    struct Trial {
+        int w, t;
+        double ms, cost, score;
+    };
+    std::vector<Trial> trials;
+    int ibest = -1;
+    for (int t : ts) {
+        for (int w : ws) {
+            if (status != CTBB_OK) break;
+            if (trials.size() >= CTBB_TUNE_MAX_TRIALS) break;
+            if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
+                status = fail(CTBB_ERR_CUDA, "autotune restore");
+                break;
+            }
+            ctbb_icd_opts c = o;
+            c.warps_in_flight = w;
+            c.lattice = t;
+            double ms_tot = 0.0;
+            for (int i = 0; i < probe_iters && status == CTBB_OK; ++i) {
+                float ms = 0.f;
+                status = launch_icd_grouped(rc, ssm, c, &ms, nullptr, nullptr);
+                ms_tot += ms;
+            }
+            if (status != CTBB_OK) break;
+            status = ctbb_gpu_recon_refresh_residual(rc, ssm);
+            double cost = 0.0;
+            if (status == CTBB_OK) status = cost_f64(rc, ssm, false, &cost);
+            if (status != CTBB_OK) break;
+            const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
+            trials.push_back({w, t, ms_tot, cost, score});
+            if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
+        }
+    }
+    if (status == CTBB_OK && copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess)
+        status = fail(CTBB_ERR_CUDA, "autotune restore");
+    if (status == CTBB_OK && cudaStreamSynchronize(st) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune sync");
+    cudaFree(d_xs);
+    cudaFree(d_es);
+    if (status != CTBB_OK) return status;
+    if (ibest < 0) return fail(CTBB_ERR_INVALID_ARG, "autotune ran no trial");
+    *best = o;
+    best->warps_in_flight = trials[ibest].w;
+    best->lattice = trials[ibest].t;
+    if (report) {
+        memset(report, 0, sizeof(*report));
+        report->n_trials = (int32_t)trials.size();
+        report->best = ibest;
+        report->start_cost = c0;
+        for (size_t i = 0; i < trials.size(); ++i) {
+            report->trials[i].warps_in_flight = trials[i].w;
+            report->trials[i].lattice = trials[i].t;
+            report->trials[i].device_ms = trials[i].ms;
+            report->trials[i].cost = trials[i].cost;
+            report->trials[i].score = trials[i].score;
+        }
+    }
+    return CTBB_OK;
+}

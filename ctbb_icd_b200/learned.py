@@ -1,0 +1,371 @@
+"""Learned warm start for grouped ICD.
+
+A small 3D residual CNN (libctbb_icd_b200: ctbb_cnn_*) is trained on pairs
+(early ICD iterate, converged ICD iterate) that the GPU ICD itself produces on
+seeded synthetic phantoms, both rotated to the fixed frame. At reconstruction
+time the network's predicted correction is added to the early iterate
+(ctbb_gpu_recon_warm_start), the voxels it moved most are revisited first
+(priority passes over ctbb_gpu_recon_set_priority's subset), and plain grouped
+ICD finishes the image. ICD from the initialize_recon_volume start remains the
+fallback and the yardstick: every result is reported with its cost and its
+RMSE in HU against the plain converged image.
+
+Device memory for the training set and crops is held in torch tensors; all
+arithmetic (ICD, rotation, the network's forward/backward passes and Adam)
+runs in the library's CUDA kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import tempfile
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import workloads as W
+from ._lib import check, lib, ptr
+
+HU = W.MU_WATER / 1000.0  # one Hounsfield unit in cm^-1
+DEFAULT_BLOCKS = 4
+S_IN = 1.0 / W.MU_WATER          # network input: water -> 1
+S_OUT = 10.0 / W.MU_WATER        # network target: 100 HU of correction -> 1
+WEIGHTS_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "weights", "warm_start.npz")
+
+
+def _dev_ptr(t) -> C.c_void_p:
+    import torch
+
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float32 and t.is_contiguous()):
+        raise TypeError("expected a contiguous float32 CUDA tensor")
+    return C.c_void_p(t.data_ptr())
+
+
+def _torch_sync():
+    import torch
+
+    torch.cuda.current_stream().synchronize()
+
+
+class WarmStartNet:
+    """Handle of the GPU network (ctbb_cnn_*). Volumes are [nz][ny][nx]
+    float32 CUDA tensors."""
+
+    def __init__(self, ctx, blocks: int = DEFAULT_BLOCKS, seed: int = 0):
+        self.ctx = ctx
+        self.blocks = int(blocks)
+        h = C.c_void_p()
+        check(lib().ctbb_cnn_create(ctx.handle, self.blocks, int(seed), C.byref(h)))
+        self.handle = h
+        self.set_scaling(S_IN, S_OUT)
+
+    @property
+    def n_params(self) -> int:
+        return int(lib().ctbb_cnn_num_params(self.handle))
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        check(lib().ctbb_cnn_get_params(self.handle, ptr(out, C.c_float), out.size))
+        return out
+
+    def set_params(self, p: np.ndarray):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        check(lib().ctbb_cnn_set_params(self.handle, ptr(p, C.c_float), p.size))
+
+    def set_scaling(self, s_in: float, s_out: float):
+        check(lib().ctbb_cnn_set_scaling(self.handle, float(s_in), float(s_out)))
+
+    def scaling(self):
+        a, b = C.c_float(), C.c_float()
+        check(lib().ctbb_cnn_get_scaling(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def forward(self, x):
+        import torch
+
+        nz, ny, nx = x.shape
+        out = torch.empty_like(x)
+        _torch_sync()
+        check(lib().ctbb_cnn_forward(self.handle, _dev_ptr(x), nx, ny, nz, _dev_ptr(out)))
+        return out
+
+    def accumulate_gradient(self, x, xc, weight=None) -> float:
+        nz, ny, nx = x.shape
+        loss = C.c_double()
+        _torch_sync()
+        check(lib().ctbb_cnn_accumulate_gradient(self.handle, _dev_ptr(x), _dev_ptr(xc),
+                                                 None if weight is None else _dev_ptr(weight),
+                                                 nx, ny, nz, C.byref(loss)))
+        return loss.value
+
+    def gradient(self) -> np.ndarray:
+        out = np.empty(self.n_params, np.float32)
+        check(lib().ctbb_cnn_get_gradient(self.handle, ptr(out, C.c_float), out.size))
+        return out
+
+    def zero_gradient(self):
+        check(lib().ctbb_cnn_zero_gradient(self.handle))
+
+    def adam_step(self, lr: float, beta1=0.9, beta2=0.999, eps=1e-8, grad_scale=1.0):
+        check(lib().ctbb_cnn_adam_step(self.handle, float(lr), float(beta1), float(beta2), float(eps),
+                                       float(grad_scale)))
+
+    def save(self, path: str, **meta):
+        s_in, s_out = self.scaling()
+        os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        np.savez(path, params=self.params(), blocks=self.blocks, s_in=s_in, s_out=s_out,
+                 **{k: np.asarray(v) for k, v in meta.items()})
+
+    @classmethod
+    def load(cls, ctx, path: str = WEIGHTS_PATH) -> "WarmStartNet":
+        d = np.load(path)
+        net = cls(ctx, int(d["blocks"]))
+        net.set_params(d["params"])
+        net.set_scaling(float(d["s_in"]), float(d["s_out"]))
+        return net
+
+    def free(self):
+        if getattr(self, "handle", None):
+            lib().ctbb_cnn_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# Scans and training pairs
+# --------------------------------------------------------------------------
+# Training geometry: cfg2's scanner, views, flying focal spot, penalty and
+# 0.6 mm voxels at the full 512 x 512 in-plane size, 8 slices per scan.
+TRAIN_WORKLOAD = "cfg2_slab"
+W.WORKLOADS[TRAIN_WORKLOAD] = dict(
+    prm={**W.WORKLOADS["cfg2"]["prm"], "Readings": 2 * 2304,
+         **W._recon(512, 30.0, 0.06, 8, -2.0, "edge-preserving", 0.1, 9.6e-4, 10)},
+    phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+)
+
+
+@dataclass
+class Scan:
+    rp: object
+    tables: object
+    rc: object
+    ssm: object
+    workdir: str
+    fov_mask: np.ndarray = field(default=None)
+
+
+def fov_mask(rp) -> np.ndarray:
+    """Voxels inside the scanner FOV (icd_iteration.cpp:181), per slice [ny][nx]."""
+    g = rp.geom
+    i = np.arange(int(g.num_voxels_x))
+    j = np.arange(int(g.num_voxels_y))
+    xx = (i[None, :] - g.center_voxel_x) * g.voxel_size_x
+    yy = (j[:, None] - g.center_voxel_y) * g.voxel_size_y
+    return (xx * xx + yy * yy) < (g.acquisition_fov / 2.0) ** 2
+
+
+def make_scan(ctx, name: str, seed: int, ssm=None, weights=None) -> Scan:
+    """A workload's geometry with phantom seed `seed`: raw data from the GPU
+    projector, zero initial image. Reuses `ssm` when given (same geometry)."""
+    import ctbb_icd_b200 as CB
+
+    w = W.workload(name)
+    w["phantom"]["seed"] = int(seed)
+    prm = w["prm"]
+    workdir = tempfile.mkdtemp(prefix="ctbb_scan_")
+    prm.update(sinogram_path=os.path.join(workdir, "raw.bin"), output_dir=workdir, output_file="out.img")
+    open(prm["sinogram_path"], "wb").close()
+    rp = CB.configure_recon_params(W.write_prm(os.path.join(workdir, "scan.prm"), prm))
+    tables = CB.slice_tables(rp)
+    spec = W.phantom_spec(w["phantom"])
+    spec.ellipsoid_z_lo = min(prm["z_start"], prm["z_end"])
+    spec.ellipsoid_z_hi = max(prm["z_start"], prm["z_end"])
+    rc = CB.Recon(rp, tables.slice_indices, ctx)
+    check(lib().ctbb_gpu_synth_raw(ctx.handle, C.byref(rp.geom), C.byref(spec), C.c_void_p(rc.raw_device_ptr())))
+    if ssm is None:
+        ssm = CB.Ssm.generate(rp, ctx, weights if weights is not None else CB.SSM_FP32)
+    rc.set_volume(ssm, None)
+    return Scan(rp, tables, rc, ssm, workdir, fov_mask(rp))
+
+
+def rmse_hu(x: np.ndarray, ref: np.ndarray, mask2d: np.ndarray) -> float:
+    d = (np.asarray(x, np.float64) - np.asarray(ref, np.float64))[:, mask2d]
+    return float(np.sqrt(np.mean(d * d)) / HU)
+
+
+def to_fixed(ctx, scan: Scan, vol: np.ndarray) -> np.ndarray:
+    import ctbb_icd_b200 as CB
+
+    out = np.ascontiguousarray(vol, dtype=np.float32).copy()
+    check(lib().ctbb_gpu_rotate(ctx.handle, C.byref(scan.rp.geom), ptr(scan.tables.tube_angles, C.c_double),
+                                ptr(scan.tables.slice_indices, C.c_uint64), ptr(out, C.c_float),
+                                CB.ROTATE_ROTATING2FIXED))
+    return out
+
+
+def converge(scan: Scan, opts, max_iter: int = 400, rel: float = 1e-7, refresh_every: int = 10):
+    """Plain grouped ICD until the FP64 cost changes by less than `rel` per
+    iteration (cost after an FP64 residual refresh every `refresh_every`
+    iterations). Returns the iterations run."""
+    prev = None
+    it = 0
+    while it < max_iter:
+        n = min(refresh_every, max_iter - it)
+        scan.rc.iterate(scan.ssm, n, opts)
+        it += n
+        scan.rc.refresh_residual(scan.ssm)
+        c = scan.rc.cost()
+        if prev is not None and abs(prev - c) / abs(c) < rel * n:
+            break
+        prev = c
+    return it
+
+
+def make_pairs(ctx, seeds, n_early: int = 3, name: str = TRAIN_WORKLOAD, opts=None, max_iter: int = 400,
+               log=print):
+    """(early iterate, converged iterate) pairs in the fixed frame, float32
+    numpy [nz][ny][nx], plus the in-FOV mask of the geometry."""
+    import ctbb_icd_b200 as CB
+
+    opts = opts or CB.icd_opts(mode=CB.ICD_GROUPED, weights=CB.SSM_FP32)
+    ssm = None
+    xs, xcs = [], []
+    mask = None
+    for s in seeds:
+        t0 = time.time()
+        scan = make_scan(ctx, name, s, ssm)
+        ssm = scan.ssm
+        scan.rc.iterate(ssm, n_early, opts)
+        x_early = scan.rc.volume()
+        n = converge(scan, opts, max_iter=max_iter)
+        xc = scan.rc.volume()
+        xs.append(to_fixed(ctx, scan, x_early))
+        xcs.append(to_fixed(ctx, scan, xc))
+        mask = scan.fov_mask
+        log(f"seed {s}: converged after {n + n_early} iterations, early->converged "
+            f"{rmse_hu(x_early, xc, scan.fov_mask):.1f} HU ({time.time() - t0:.1f} s)")
+        scan.rc.free()
+    return np.stack(xs), np.stack(xcs), mask
+
+
+def train(net: WarmStartNet, x_early: np.ndarray, x_conv: np.ndarray, mask2d: np.ndarray, steps: int = 1500,
+          batch: int = 4, crop=(8, 128, 128), lr: float = 1e-3, lr_min: float = 1e-4, seed: int = 0,
+          log=print, log_every: int = 100):
+    """Adam on random crops of the training pairs (cosine learning-rate decay)."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    X = torch.from_numpy(np.ascontiguousarray(x_early, np.float32)).to(dev)
+    Y = torch.from_numpy(np.ascontiguousarray(x_conv, np.float32)).to(dev)
+    M = torch.from_numpy(mask2d.astype(np.float32)).to(dev)
+    n, nz, ny, nx = X.shape
+    cz, cy, cx = min(crop[0], nz), min(crop[1], ny), min(crop[2], nx)
+    g = np.random.default_rng(seed)
+    hist = []
+    for step in range(steps):
+        loss = 0.0
+        for _ in range(batch):
+            i = int(g.integers(n))
+            z = int(g.integers(nz - cz + 1))
+            y = int(g.integers(ny - cy + 1))
+            x = int(g.integers(nx - cx + 1))
+            xb = X[i, z:z + cz, y:y + cy, x:x + cx].contiguous()
+            yb = Y[i, z:z + cz, y:y + cy, x:x + cx].contiguous()
+            mb = M[y:y + cy, x:x + cx].expand(cz, cy, cx).contiguous()
+            if float(mb.sum()) == 0.0:
+                mb = torch.ones_like(mb)
+            loss += net.accumulate_gradient(xb, yb, mb)
+        lr_t = lr_min + 0.5 * (lr - lr_min) * (1 + np.cos(np.pi * step / max(1, steps)))
+        net.adam_step(lr_t, grad_scale=1.0 / batch)
+        hist.append(loss / batch)
+        if log and (step % log_every == 0 or step == steps - 1):
+            log(f"step {step}: loss {np.mean(hist[-log_every:]):.5f} lr {lr_t:.2e}")
+    return hist
+
+
+def eval_loss(net: WarmStartNet, x_early: np.ndarray, x_conv: np.ndarray, mask2d: np.ndarray) -> float:
+    """Mean weighted loss over whole volumes (the gradient buffer is cleared)."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    M = torch.from_numpy(mask2d.astype(np.float32)).to(dev)
+    tot = 0.0
+    for xe, xc in zip(x_early, x_conv):
+        xb = torch.from_numpy(np.ascontiguousarray(xe, np.float32)).to(dev)
+        yb = torch.from_numpy(np.ascontiguousarray(xc, np.float32)).to(dev)
+        tot += net.accumulate_gradient(xb, yb, M.expand(*xb.shape).contiguous())
+    net.zero_gradient()
+    return tot / len(x_early)
+
+
+# --------------------------------------------------------------------------
+# Time to <= tol HU: plain vs learned warm start
+# --------------------------------------------------------------------------
+def _timed(fn):
+    import torch
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    r = fn()
+    torch.cuda.synchronize()
+    return r, time.perf_counter() - t0
+
+
+def time_to_tolerance(scan: Scan, x_ref: np.ndarray, opts, tol_hu: float = 0.5, max_iter: int = 200,
+                      net: WarmStartNet | None = None, n_early: int = 3, prio_fraction: float = 0.2,
+                      prio_passes: int = 2, refresh_every: int = 10):
+    """Iterate from the zero start until RMSE(x, x_ref) <= tol_hu inside the
+    FOV. With `net`, after n_early plain iterations the warm start is applied
+    and `prio_passes` passes over the top `prio_fraction` voxels run before
+    plain iterations resume. Returns the wall time of the reconstruction work
+    (RMSE checks excluded), the full iterations run and the trace."""
+    import ctbb_icd_b200 as CB
+
+    scan.rc.set_volume(scan.ssm, None)
+    elapsed = 0.0
+    trace = []
+    it = 0
+
+    def check_done(label):
+        x = scan.rc.volume()
+        e = rmse_hu(x, x_ref, scan.fov_mask)
+        trace.append((label, elapsed, e))
+        return e <= tol_hu
+
+    if net is not None:
+        _, dt = _timed(lambda: scan.rc.iterate(scan.ssm, n_early, opts))
+        elapsed += dt
+        it += n_early
+        check_done(f"plain x{n_early}")
+        _, dt = _timed(lambda: scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles))
+        elapsed += dt
+        done = check_done("warm start")
+        if not done and prio_passes > 0 and prio_fraction > 0:
+            popts = CB.icd_opts(mode=opts.mode, weights=opts.weights, warps_in_flight=opts.warps_in_flight,
+                                lattice=opts.lattice, relax=opts.relax, priority=True)
+            _, dt = _timed(lambda: (scan.rc.set_priority(prio_fraction, popts),
+                                    scan.rc.iterate(scan.ssm, prio_passes, popts)))
+            elapsed += dt
+            done = check_done(f"priority x{prio_passes} @ {prio_fraction}")
+        if done:
+            return {"seconds": elapsed, "iterations": it, "trace": trace, "reached": True}
+    while it < max_iter:
+        refresh = refresh_every > 0 and it > 0 and it % refresh_every == 0
+
+        def step():
+            if refresh:
+                scan.rc.refresh_residual(scan.ssm)
+            return scan.rc.iterate(scan.ssm, 1, opts)
+
+        _, dt = _timed(step)
+        elapsed += dt
+        it += 1
+        if check_done(f"iter {it}"):
+            return {"seconds": elapsed, "iterations": it, "trace": trace, "reached": True}
+    return {"seconds": elapsed, "iterations": it, "trace": trace, "reached": False}

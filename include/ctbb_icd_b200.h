@@ -271,6 +271,9 @@ typedef struct ctbb_icd_opts {
     int32_t compute_cost;     /* evaluate the FP64 cost after each iteration      */
     double stop_rel_change;   /* stop when |dcost|/cost < this (0: fixed count)   */
     double relax;             /* grouped: step scale omega in (0, 2) (0: 1.0)     */
+    int32_t priority;         /* grouped: visit only the priority subset built by
+                                 ctbb_gpu_recon_set_priority (0: every voxel)     */
+    int32_t reserved2;
 } ctbb_icd_opts;
 
 typedef struct ctbb_iter_stats {
@@ -381,6 +384,77 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
                                            const double* tube_angles_deg,
                                            const uint64_t* slice_indices, const float* in_dev,
                                            float* out_dev, int32_t direction);
+
+/*
+ * Autotuner for grouped ICD (no reference counterpart). From the current
+ * iterate, runs probe_iters iterations for each candidate pair (warps in
+ * flight, tile edge of the visiting order) and keeps the pair with the
+ * largest decrease of the FP64 cost per millisecond of device time. The
+ * iterate and e are restored afterwards; *best = *base with the two fields
+ * set. Candidates: 1, 2, 4, ..., 32 times the coupling-bound default of
+ * warps (at most 48 per SM) and tile edges nx/16, nx/8, nx/4.
+ */
+#define CTBB_TUNE_MAX_TRIALS 32
+typedef struct ctbb_tune_trial {
+    int32_t warps_in_flight;
+    int32_t lattice;
+    double device_ms;   /* ICD kernel time of the probe iterations */
+    double cost;        /* FP64 cost after them                    */
+    double score;       /* (start_cost - cost) / device_ms         */
+} ctbb_tune_trial;
+typedef struct ctbb_tune_report {
+    int32_t n_trials;
+    int32_t best;       /* index into trials */
+    double start_cost;
+    ctbb_tune_trial trials[CTBB_TUNE_MAX_TRIALS];
+} ctbb_tune_report;
+ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts* base,
+                                    int32_t probe_iters, ctbb_icd_opts* best, ctbb_tune_report* report);
+
+/*
+ * Learned warm start (no reference counterpart). A 3D residual CNN with 32
+ * channels, `blocks` residual blocks and 3x3x3 kernels predicts, from an
+ * early ICD iterate in the fixed frame, the correction to the converged
+ * image. Training and inference run on the GPU (BF16 tensor-core
+ * convolutions with FP32 accumulation, Adam on FP32 master weights).
+ *
+ * Parameter layout (flat FP32): W_in[27][32], b_in[32]; per block
+ * W1[27][32][32] (tap, in, out), b1[32], W2[27][32][32], b2[32];
+ * W_out[27][32], b_out[1]. Tap t = (dz+1)*9 + (dy+1)*3 + (dx+1).
+ * Scaling: the network sees s_in * x and is trained on (x_conv - x) * s_out.
+ * Volumes are device float arrays [nz][ny][nx] on the context's device.
+ */
+typedef struct ctbb_cnn ctbb_cnn;
+ctbb_status ctbb_cnn_create(ctbb_ctx* ctx, int32_t blocks, uint64_t seed, ctbb_cnn** out);
+void ctbb_cnn_free(ctbb_cnn* cnn);
+uint64_t ctbb_cnn_num_params(const ctbb_cnn* cnn);
+ctbb_status ctbb_cnn_get_params(ctbb_cnn* cnn, float* params_host, uint64_t n);
+ctbb_status ctbb_cnn_set_params(ctbb_cnn* cnn, const float* params_host, uint64_t n);
+ctbb_status ctbb_cnn_set_scaling(ctbb_cnn* cnn, float s_in, float s_out);
+ctbb_status ctbb_cnn_get_scaling(const ctbb_cnn* cnn, float* s_in, float* s_out);
+/* Network output (predicted (x_conv - x) * s_out) for x_dev. */
+ctbb_status ctbb_cnn_forward(ctbb_cnn* cnn, const float* x_dev, int32_t nx, int32_t ny, int32_t nz,
+                             float* out_dev);
+/* Adds d loss / d params to the gradient buffer, where loss =
+ * sum w (out - (xc - x) s_out)^2 / sum w (weight_dev NULL: w = 1). */
+ctbb_status ctbb_cnn_accumulate_gradient(ctbb_cnn* cnn, const float* x_dev, const float* xc_dev,
+                                         const float* weight_dev, int32_t nx, int32_t ny, int32_t nz,
+                                         double* loss);
+ctbb_status ctbb_cnn_get_gradient(ctbb_cnn* cnn, float* grad_host, uint64_t n);
+ctbb_status ctbb_cnn_zero_gradient(ctbb_cnn* cnn);
+/* One Adam step on grad * grad_scale; clears the gradient buffer. */
+ctbb_status ctbb_cnn_adam_step(ctbb_cnn* cnn, float lr, float beta1, float beta2, float eps, float grad_scale);
+
+/* Apply the network to the current iterate: rotate to the fixed frame
+ * (rotate_slices_rotating2fixed, rotate_slices.cpp:81-114), predict the
+ * correction, rotate it back (rotate_slices_fixed2rotating, :48-79), add it
+ * with the positivity clamp, recompute e = y - Ax in FP64, and keep
+ * |step| per voxel as the priority map. tube_angles_deg: ct_data.tube_angles. */
+ctbb_status ctbb_gpu_recon_warm_start(ctbb_recon* rc, const ctbb_ssm* ssm, ctbb_cnn* cnn,
+                                      const double* tube_angles_deg);
+/* Restrict priority passes (opts->priority = 1) to the `fraction` of voxels
+ * with the largest warm-start step, kept in the visiting order of opts. */
+ctbb_status ctbb_gpu_recon_set_priority(ctbb_recon* rc, const ctbb_icd_opts* opts, double fraction);
 
 #ifdef __cplusplus
 }
