@@ -130,6 +130,8 @@ def setup_workload(ctx, workdir, seed, weights, name=WORKLOAD):
     spec = W.phantom_spec(w["phantom"])
     spec.ellipsoid_z_lo = min(prm["z_start"], prm["z_end"])
     spec.ellipsoid_z_hi = max(prm["z_start"], prm["z_end"])
+    # Phantom cut to the reconstructed slab: data consistent with the model.
+    spec.clip_z_lo, spec.clip_z_hi = W.slab_clip(rp, tables.slice_locations)
     rc = C.Recon(rp, tables.slice_indices, ctx)
     C.check(C.lib().ctbb_gpu_synth_raw(ctx.handle, ctypes.byref(rp.geom), ctypes.byref(spec),
                                        ctypes.c_void_p(rc.raw_device_ptr())))
@@ -158,8 +160,17 @@ def run_ours(args, rank, world, dist):
                                          name=args.workload)
     setup_s = time.time() - t0
     info = ssm.info()
-    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice,
+                      warps_per_voxel=args.wpv)
     nvox = int(np.prod(rp.shape))
+    tune = None
+    if args.autotune:
+        # Probe from an early iterate, as a user would before a long run.
+        rc.iterate(ssm, 3, opts)
+        opts, trials = rc.autotune(ssm, opts, probe_iters=2)
+        tune = {"chosen": {"warps_per_voxel": opts.warps_per_voxel, "warps_in_flight": opts.warps_in_flight,
+                           "lattice": opts.lattice}, "trials": len(trials)}
+        rc.set_volume(ssm, None)
 
     # Algorithmic bytes per iteration (one launch): e read + written once per
     # in-range entry (8 B), the SSM read once (index + weight), image r+w.
@@ -220,14 +231,17 @@ def run_ours(args, rank, world, dist):
                 "weights": args.weights, "error_sinogram": "fp32", "voxels": nvox,
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
-                "warps_in_flight": args.warps or "auto", "l2": "inputs larger than L2 (e 1.74 GB, SSM > 20 GB)",
+                "warps_in_flight": opts.warps_in_flight or "auto", "warps_per_voxel": max(1, opts.warps_per_voxel),
+                "lattice": opts.lattice or "auto", "autotune": tune,
+                "l2": "inputs larger than L2 (e 1.74 GB, SSM > 20 GB)",
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                 "setup_s": round(setup_s, 1),
             },
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "icd_grouped_kernel", "algorithmic_bytes_per_launch": b_iter,
+                "kernel": "icd_grouped_kernel" if opts.warps_per_voxel <= 1 else "icd_cta_kernel",
+                "algorithmic_bytes_per_launch": b_iter,
                 "kernel_ms_per_launch": kernel_ms_per_launch, "peak_source": peak_kind,
             },
             "gpu_launches": int(args.steps),
@@ -462,6 +476,9 @@ def main():
                     help="workload name from ctbb_icd_b200.workloads (the benchmark is cfg2)")
     ap.add_argument("--warps", type=int, default=0, help="warps in flight (0: auto)")
     ap.add_argument("--lattice", type=int, default=0)
+    ap.add_argument("--wpv", type=int, default=1, help="warps per voxel update: 1, 4 or 8")
+    ap.add_argument("--autotune", action="store_true", help="pick warps per voxel, warps in flight and tile "
+                    "edge with the library's autotuner before timing")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=10, help="ICD iterations per drop-in call")

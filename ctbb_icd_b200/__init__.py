@@ -251,13 +251,15 @@ class Ssm:
 
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
-             compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False) -> IcdOpts:
+             compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False,
+             warps_per_voxel=1) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
     o.compute_cost, o.stop_rel_change = int(bool(compute_cost)), float(stop_rel_change)
     o.relax = float(relax)
     o.priority = int(bool(priority))
+    o.warps_per_voxel = int(warps_per_voxel)
     return o
 
 
@@ -331,7 +333,8 @@ class Recon:
         best, rep = IcdOpts(), TuneReport()
         check(lib().ctbb_gpu_recon_autotune(self.handle, ssm.handle, C.byref(opts or icd_opts()),
                                             int(probe_iters), C.byref(best), C.byref(rep)))
-        trials = [dict(warps_in_flight=t.warps_in_flight, lattice=t.lattice, device_ms=t.device_ms,
+        trials = [dict(warps_in_flight=t.warps_in_flight, warps_per_voxel=t.warps_per_voxel,
+                       lattice=t.lattice, device_ms=t.device_ms,
                        cost=t.cost, score=t.score, best=(i == rep.best))
                   for i, t in enumerate(rep.trials[:rep.n_trials])]
         return best, trials

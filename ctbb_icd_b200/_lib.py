@@ -84,7 +84,7 @@ class PrmStrings(C.Structure):
 class PhantomSpec(C.Structure):
     _fields_ = [
         ("n_ellipsoids", _I), ("reserved", _I), ("seed", _U), ("ellipsoid_z_lo", _D),
-        ("ellipsoid_z_hi", _D), ("i0_lo", _D), ("i0_hi", _D),
+        ("ellipsoid_z_hi", _D), ("i0_lo", _D), ("i0_hi", _D), ("clip_z_lo", _D), ("clip_z_hi", _D),
     ]
 
 
@@ -99,12 +99,13 @@ class IcdOpts(C.Structure):
     _fields_ = [
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
-        ("priority", _I), ("reserved2", _I),
+        ("priority", _I), ("warps_per_voxel", _I),
     ]
 
 
 class TuneTrial(C.Structure):
-    _fields_ = [("warps_in_flight", _I), ("lattice", _I), ("device_ms", _D), ("cost", _D), ("score", _D)]
+    _fields_ = [("warps_in_flight", _I), ("warps_per_voxel", _I), ("lattice", _I), ("reserved", _I),
+                ("device_ms", _D), ("cost", _D), ("score", _D)]
 
 
 class TuneReport(C.Structure):

@@ -114,14 +114,15 @@ constexpr int kMaxObjects = 96;
 __constant__ ctbb_object c_objects[kMaxObjects];
 
 __global__ void __launch_bounds__(256) synth_kernel(ctbb_ray_geom G, int n_obj, uint64_t seed, double i0_lo,
-                                                    double i0_hi, float* __restrict__ raw) {
+                                                    double i0_hi, double clip_lo, double clip_hi,
+                                                    float* __restrict__ raw) {
     const uint64_t n = (uint64_t)G.readings * G.n_channels * G.n_rows;
     for (uint64_t ray = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; ray < n;
          ray += (uint64_t)gridDim.x * blockDim.x) {
         const int64_t r = (int64_t)(ray % G.n_rows);
         const int64_t c = (int64_t)((ray / G.n_rows) % G.n_channels);
         const int64_t v = (int64_t)(ray / ((uint64_t)G.n_rows * G.n_channels));
-        const double p = ctbb_line_integral(G, c_objects, n_obj, v, c, r);
+        const double p = ctbb_line_integral(G, c_objects, n_obj, v, c, r, clip_lo, clip_hi);
         raw[ray] = ctbb_noisy_sample(p, ctbb_view_i0(seed, v, i0_lo, i0_hi), seed, ray);
     }
 }
@@ -150,7 +151,8 @@ extern "C" ctbb_status ctbb_gpu_synth_raw(ctbb_ctx* ctx, const ctbb_geom_c* geom
     const ctbb_ray_geom G = ctbb_ray_geom_from(g);
     const uint64_t n = (uint64_t)G.readings * G.n_channels * G.n_rows;
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 32));
-    synth_kernel<<<grid, 256, 0, ctx->stream>>>(G, (int)objs.size(), spec->seed, spec->i0_lo, spec->i0_hi, raw_dev);
+    synth_kernel<<<grid, 256, 0, ctx->stream>>>(G, (int)objs.size(), spec->seed, spec->i0_lo, spec->i0_hi,
+                                                spec->clip_z_lo, spec->clip_z_hi, raw_dev);
     CTBB_CUDA(cudaGetLastError());
     CTBB_CUDA(cudaStreamSynchronize(ctx->stream));
     return CTBB_OK;

@@ -292,6 +292,120 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
     }
 }
 
+// CTA-per-voxel variant: WPV warps share one voxel update. Each thread keeps
+// up to R of the item's entries (sinogram index and weight) in registers
+// from the gather to the scatter, so the matrix column is read from memory
+// once per update and the reductions hit e's lines while they are still in
+// L2; with one item per CTA, one to a few updates per SM are in flight.
+// Entries beyond 32 * WPV * R (rare) are streamed twice.
+template <class WT, int WPV, int R>
+__global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint32_t* __restrict__ order,
+                                                        const int64_t* __restrict__ colptr,
+                                                        const uint32_t* __restrict__ vptr,
+                                                        const int32_t* __restrict__ idx, const WT* __restrict__ w,
+                                                        const int32_t* __restrict__ start, float* e, float* x,
+                                                        unsigned long long* queue) {
+    constexpr int NT = 32 * WPV;
+    constexpr int64_t CAP = (int64_t)NT * R;
+    __shared__ unsigned long long s_item;
+    __shared__ float s_red[2 * WPV + 1];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(queue, 1ull);
+        __syncthreads();
+        const uint64_t item = s_item;
+        if (item >= P.n_items) break;
+        const uint32_t packed = __ldg(order + item);
+        const uint64_t col = packed / (uint32_t)P.nz;
+        const int k = (int)(packed % (uint32_t)P.nz);
+        const int64_t q = (int64_t)col + (int64_t)ncol * k;
+        const int s = start[k];
+        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+        int64_t b = 0, en = 0;
+        if (v1 > v0) {
+            const int64_t cb = colptr[col];
+            const uint32_t* vp = vptr + col * P.nvsm1;
+            b = cb + vp[v0];
+            en = cb + vp[v1];
+        }
+        const int off = s * P.nch * P.nr;
+        const int64_t e0 = min(en, b + CAP);
+        int qr[R];
+        float wr[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t m = b + tid + (int64_t)NT * r;
+            if (m < e0) {
+                qr[r] = __ldg(idx + m) + off;
+                wr[r] = ldw(w, m);
+            } else {
+                qr[r] = -1;
+                wr[r] = 0.f;
+            }
+        }
+        float acc_b = 0.f, acc_a = 0.f;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const float ev = qr[r] >= 0 ? __ldcg(e + qr[r]) : 0.f;
+            acc_b = fmaf(wr[r], ev, acc_b);
+            acc_a = fmaf(wr[r], wr[r], acc_a);
+        }
+        for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+            int qo[kU];
+            float wo[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int64_t m = base + tid + (int64_t)NT * u;
+                qo[u] = m < en ? __ldg(idx + m) + off : -1;
+                wo[u] = m < en ? ldw(w, m) : 0.f;
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const float ev = qo[u] >= 0 ? __ldcg(e + qo[u]) : 0.f;
+                acc_b = fmaf(wo[u], ev, acc_b);
+                acc_a = fmaf(wo[u], wo[u], acc_a);
+            }
+        }
+        acc_b = warp_sum(acc_b);
+        acc_a = warp_sum(acc_a);
+        if (lane == 0) {
+            s_red[wid] = acc_b;
+            s_red[WPV + wid] = acc_a;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            double beta = 0.0, alpha = 0.0;
+#pragma unroll
+            for (int i = 0; i < WPV; ++i) {
+                beta += (double)s_red[i];
+                alpha += (double)s_red[WPV + i];
+            }
+            const double xq = (double)__ldcg(x + q);
+            double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+            if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+            if (lane == 0) {
+                x[q] = (float)(xq + upd);
+                s_red[2 * WPV] = (float)upd;
+            }
+        }
+        __syncthreads();
+        const float du = s_red[2 * WPV];
+        if (du != 0.f) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (qr[r] >= 0) atomicAdd(e + qr[r], -du * wr[r]);
+            for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int64_t m = base + tid + (int64_t)NT * u;
+                    if (m < en) atomicAdd(e + (__ldg(idx + m) + off), -du * ldw(w, m));
+                }
+            }
+        }
+    }
+}
+
 // Batched variant: one persistent launch drains the merged queue of several
 // independent scans (`merged[t]` = scan << 40 | item within that scan).
 template <class WT>
@@ -578,7 +692,9 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
         if (prio && rc->n_order > 0) *entries *= (double)rc->n_prio_order / (double)rc->n_order;
     }
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
-    const int blocks = std::max(1, (W + 7) / 8);
+    const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
+    if (wpv != 1 && wpv != 4 && wpv != 8)
+        return fail(CTBB_ERR_INVALID_ARG, "warps_per_voxel must be 1, 4 or 8 (got %d)", wpv);
     ctbb_ctx* ctx = rc->ctx;
     cudaStream_t st = ctx->stream;
     CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), st));
@@ -587,14 +703,37 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     CTBB_CUDA(cudaEventCreate(&e1));
     CTBB_CUDA(cudaEventRecord(e0, st));
     const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
-    if (wsel == CTBB_SSM_FP16)
-        icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
-                                                           ssm->d_w16, rc->d_start, rc->d_e32, rc->d_x32,
-                                                           ctx->d_queue);
-    else
-        icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx,
-                                                          ssm->d_w32, rc->d_start, rc->d_e32, rc->d_x32,
-                                                          ctx->d_queue);
+    const bool h = wsel == CTBB_SSM_FP16;
+    const int64_t* cp = ssm->d_colptr;
+    const uint32_t* vp = ssm->d_vptr;
+    const int32_t* ix = ssm->d_idx;
+    if (wpv == 1) {
+        const int blocks = std::max(1, (W + 7) / 8);
+        if (h)
+            icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                               rc->d_e32, rc->d_x32, ctx->d_queue);
+        else
+            icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                              rc->d_e32, rc->d_x32, ctx->d_queue);
+    } else {
+        // warps_in_flight counts warps: W / wpv voxel updates in flight.
+        const int blocks = std::max(1, W / wpv);
+        if (wpv == 8) {
+            if (h)
+                icd_cta_kernel<__half, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+            else
+                icd_cta_kernel<float, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+        } else {
+            if (h)
+                icd_cta_kernel<__half, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+            else
+                icd_cta_kernel<float, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+        }
+    }
     CTBB_CUDA(cudaGetLastError());
     CTBB_CUDA(cudaEventRecord(e1, st));
     CTBB_CUDA(cudaEventSynchronize(e1));

@@ -129,7 +129,10 @@ struct ctbb_object {
     double value;      // additive attenuation (cm^-1)
 };
 
-CTBB_HD double ctbb_object_chord(const ctbb_object& o, const double s[3], const double u[3]) {
+// Parameter interval [*t0, *t1] of the unit ray s + t u inside the object;
+// returns false when the ray misses it.
+CTBB_HD bool ctbb_object_interval(const ctbb_object& o, const double s[3], const double u[3], double* t0,
+                                  double* t1) {
     double A, B, C;
     if (o.kind == CTBB_OBJ_ZCYLINDER) {
         const double dx = s[0] - o.c[0], dy = s[1] - o.c[1];
@@ -149,10 +152,20 @@ CTBB_HD double ctbb_object_chord(const ctbb_object& o, const double s[3], const 
         B = 2.0 * (p[0] * q[0] + p[1] * q[1] + p[2] * q[2]);
         C = p[0] * p[0] + p[1] * p[1] + p[2] * p[2] - 1.0;
     }
-    if (A <= 0.0) return 0.0;
+    if (A <= 0.0) return false;
     const double disc = B * B - 4.0 * A * C;
-    if (disc <= 0.0) return 0.0;
-    return sqrt(disc) / A;  // |u| = 1, so the parameter span is the chord length
+    if (disc <= 0.0) return false;
+    const double h = sqrt(disc);
+    *t0 = (-B - h) / (2.0 * A);
+    *t1 = (-B + h) / (2.0 * A);
+    return true;
+}
+
+// Chord length of the unit ray inside the object (the parameter span, |u| = 1).
+CTBB_HD double ctbb_object_chord(const ctbb_object& o, const double s[3], const double u[3]) {
+    double t0, t1;
+    if (!ctbb_object_interval(o, s, u, &t0, &t1)) return 0.0;
+    return t1 - t0;
 }
 
 // Scanner/ray geometry needed by the projector (derived recon_params values).
@@ -189,13 +202,35 @@ CTBB_HD void ctbb_ray(const ctbb_ray_geom& G, int64_t g, int64_t j, int64_t r, d
     u[2] = d2 / n;
 }
 
-// Noise-free line integral of the phantom along ray (g, j, r).
+// Noise-free line integral of the phantom along ray (g, j, r). With
+// clip_hi > clip_lo every object is cut to the slab clip_lo <= z <= clip_hi
+// (a phantom of finite length).
 CTBB_HD double ctbb_line_integral(const ctbb_ray_geom& G, const ctbb_object* objs, int n_obj,
-                                  int64_t g, int64_t j, int64_t r) {
+                                  int64_t g, int64_t j, int64_t r, double clip_lo = 0.0, double clip_hi = 0.0) {
     double s[3], u[3];
     ctbb_ray(G, g, j, r, s, u);
+    double zt0 = -INFINITY, zt1 = INFINITY;
+    if (clip_hi > clip_lo) {
+        if (u[2] != 0.0) {
+            const double a = (clip_lo - s[2]) / u[2], b = (clip_hi - s[2]) / u[2];
+            zt0 = a < b ? a : b;
+            zt1 = a < b ? b : a;
+        } else if (s[2] < clip_lo || s[2] > clip_hi) {
+            return 0.0;
+        }
+    }
     double p = 0.0;
-    for (int k = 0; k < n_obj; ++k) p += objs[k].value * ctbb_object_chord(objs[k], s, u);
+    for (int k = 0; k < n_obj; ++k) {
+        double t0, t1;
+        if (!ctbb_object_interval(objs[k], s, u, &t0, &t1)) continue;
+        if (!(clip_hi > clip_lo)) {
+            p += objs[k].value * (t1 - t0);
+            continue;
+        }
+        t0 = t0 > zt0 ? t0 : zt0;
+        t1 = t1 < zt1 ? t1 : zt1;
+        if (t1 > t0) p += objs[k].value * (t1 - t0);
+    }
     return p;
 }
 

@@ -47,15 +47,20 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     ctbb_status status = CTBB_OK;
     if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
 
-    // Candidates: multiples of the coupling-bound default, and tile edges of
-    // 1/16, 1/8 and 1/4 of the slice.
+    // Candidates (warps per voxel, warps in flight): one warp per voxel at
+    // multiples of the coupling-bound default; 8 warps per voxel with one or
+    // two updates per SM; 4 warps per voxel with two or four per SM. Tile
+    // edges of 1/16, 1/8 and 1/4 of the slice.
     const int w0 = default_warps_in_flight(rc);
-    const int wmax = rc->ctx->sm_count * 48;
-    std::vector<int> ws;
+    const int sms = rc->ctx->sm_count;
+    const int wmax = sms * 48;
+    std::vector<std::pair<int, int>> ws;
     for (int m : {1, 2, 4, 8, 16, 32}) {
         const int w = std::max(32, std::min(wmax, w0 * m));
-        if (std::find(ws.begin(), ws.end(), w) == ws.end()) ws.push_back(w);
+        if (std::find(ws.begin(), ws.end(), std::make_pair(1, w)) == ws.end()) ws.push_back({1, w});
     }
+    for (int per_sm : {1, 2}) ws.push_back({8, 8 * sms * per_sm});
+    for (int per_sm : {2, 4}) ws.push_back({4, 4 * sms * per_sm});
     const int nx = (int)rc->geom.num_voxels_x;
     std::vector<int> ts;
     for (int d : {16, 8, 4}) {
@@ -63,13 +68,14 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
         if (std::find(ts.begin(), ts.end(), t) == ts.end()) ts.push_back(t);
     }
     struct Trial {
-        int w, t;
+        int wpv, w, t;
         double ms, cost, score;
     };
     std::vector<Trial> trials;
     int ibest = -1;
     for (int t : ts) {
-        for (int w : ws) {
+        for (const auto& pw : ws) {
+            const int wpv = pw.first, w = pw.second;
             if (status != CTBB_OK) break;
             if (trials.size() >= CTBB_TUNE_MAX_TRIALS) break;
             if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
@@ -78,6 +84,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             }
             ctbb_icd_opts c = o;
             c.warps_in_flight = w;
+            c.warps_per_voxel = wpv;
             c.lattice = t;
             double ms_tot = 0.0;
             for (int i = 0; i < probe_iters && status == CTBB_OK; ++i) {
@@ -91,7 +98,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             if (status == CTBB_OK) status = cost_f64(rc, ssm, false, &cost);
             if (status != CTBB_OK) break;
             const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
-            trials.push_back({w, t, ms_tot, cost, score});
+            trials.push_back({wpv, w, t, ms_tot, cost, score});
             if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
         }
     }
@@ -104,6 +111,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     if (ibest < 0) return fail(CTBB_ERR_INVALID_ARG, "autotune ran no trial");
     *best = o;
     best->warps_in_flight = trials[ibest].w;
+    best->warps_per_voxel = trials[ibest].wpv;
     best->lattice = trials[ibest].t;
     if (report) {
         memset(report, 0, sizeof(*report));
@@ -112,6 +120,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
         report->start_cost = c0;
         for (size_t i = 0; i < trials.size(); ++i) {
             report->trials[i].warps_in_flight = trials[i].w;
+            report->trials[i].warps_per_voxel = trials[i].wpv;
             report->trials[i].lattice = trials[i].t;
             report->trials[i].device_ms = trials[i].ms;
             report->trials[i].cost = trials[i].cost;

@@ -141,13 +141,22 @@ class WarmStartNet:
 # Scans and training pairs
 # --------------------------------------------------------------------------
 # Training geometry: cfg2's scanner, views, flying focal spot, penalty and
-# 0.6 mm voxels at the full 512 x 512 in-plane size, 8 slices per scan.
+# 0.6 mm voxels at the full 512 x 512 in-plane size, 16 slices per scan.
 TRAIN_WORKLOAD = "cfg2_slab"
 W.WORKLOADS[TRAIN_WORKLOAD] = dict(
     prm={**W.WORKLOADS["cfg2"]["prm"], "Readings": 2 * 2304,
-         **W._recon(512, 30.0, 0.06, 8, -2.0, "edge-preserving", 0.1, 9.6e-4, 10)},
+         **W._recon(512, 30.0, 0.06, 16, -2.0, "edge-preserving", 0.1, 9.6e-4, 10)},
     phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
 )
+# A phantom longer than the reconstructed slab makes the data inconsistent
+# with the slab model: rays that leave the slab carry attenuation that ICD
+# (the reference's and this one) can only place on in-slab voxels, and it
+# lands in the grid-edge rows of the outer slices. Scans here cut the phantom
+# to the slab (make_scan's clip); error figures also stay inside the object
+# support (r < OBJECT_RADIUS_CM; the phantom reaches 12 cm) and skip
+# EDGE_SLICES slices at each end.
+OBJECT_RADIUS_CM = 13.0
+EDGE_SLICES = 2
 
 
 @dataclass
@@ -158,6 +167,11 @@ class Scan:
     ssm: object
     workdir: str
     fov_mask: np.ndarray = field(default=None)
+    obj_mask: np.ndarray = field(default=None)
+
+    def error_hu(self, x: np.ndarray, ref: np.ndarray) -> float:
+        """RMSE in HU inside the object support on the interior slices."""
+        return rmse_hu(x, ref, self.obj_mask, interior(x.shape[0]))
 
 
 def fov_mask(rp) -> np.ndarray:
@@ -170,9 +184,10 @@ def fov_mask(rp) -> np.ndarray:
     return (xx * xx + yy * yy) < (g.acquisition_fov / 2.0) ** 2
 
 
-def make_scan(ctx, name: str, seed: int, ssm=None, weights=None) -> Scan:
+def make_scan(ctx, name: str, seed: int, ssm=None, weights=None, clip: bool = True) -> Scan:
     """A workload's geometry with phantom seed `seed`: raw data from the GPU
-    projector, zero initial image. Reuses `ssm` when given (same geometry)."""
+    projector (phantom cut to the reconstructed slab unless clip=False), zero
+    initial image. Reuses `ssm` when given (same geometry)."""
     import ctbb_icd_b200 as CB
 
     w = W.workload(name)
@@ -186,16 +201,37 @@ def make_scan(ctx, name: str, seed: int, ssm=None, weights=None) -> Scan:
     spec = W.phantom_spec(w["phantom"])
     spec.ellipsoid_z_lo = min(prm["z_start"], prm["z_end"])
     spec.ellipsoid_z_hi = max(prm["z_start"], prm["z_end"])
+    if clip:
+        spec.clip_z_lo, spec.clip_z_hi = W.slab_clip(rp, tables.slice_locations)
     rc = CB.Recon(rp, tables.slice_indices, ctx)
     check(lib().ctbb_gpu_synth_raw(ctx.handle, C.byref(rp.geom), C.byref(spec), C.c_void_p(rc.raw_device_ptr())))
     if ssm is None:
         ssm = CB.Ssm.generate(rp, ctx, weights if weights is not None else CB.SSM_FP32)
     rc.set_volume(ssm, None)
-    return Scan(rp, tables, rc, ssm, workdir, fov_mask(rp))
+    return Scan(rp, tables, rc, ssm, workdir, fov_mask(rp), object_mask(rp))
 
 
-def rmse_hu(x: np.ndarray, ref: np.ndarray, mask2d: np.ndarray) -> float:
-    d = (np.asarray(x, np.float64) - np.asarray(ref, np.float64))[:, mask2d]
+def object_mask(rp, radius_cm: float = OBJECT_RADIUS_CM) -> np.ndarray:
+    """In-plane disc [ny][nx] of radius `radius_cm` about the rotation axis."""
+    g = rp.geom
+    i = np.arange(int(g.num_voxels_x))
+    j = np.arange(int(g.num_voxels_y))
+    xx = (i[None, :] - g.center_voxel_x) * g.voxel_size_x
+    yy = (j[:, None] - g.center_voxel_y) * g.voxel_size_y
+    return (xx * xx + yy * yy) < radius_cm * radius_cm
+
+
+def interior(nz: int, edge: int = EDGE_SLICES) -> slice:
+    e = edge if nz > 2 * edge else 0
+    return slice(e, nz - e)
+
+
+def rmse_hu(x: np.ndarray, ref: np.ndarray, mask2d: np.ndarray, slices: slice | None = None) -> float:
+    """RMSE in HU over mask2d on every slice (or the given slices)."""
+    d = (np.asarray(x, np.float64) - np.asarray(ref, np.float64))
+    if slices is not None:
+        d = d[slices]
+    d = d[:, mask2d]
     return float(np.sqrt(np.mean(d * d)) / HU)
 
 
@@ -230,7 +266,8 @@ def converge(scan: Scan, opts, max_iter: int = 400, rel: float = 1e-7, refresh_e
 def make_pairs(ctx, seeds, n_early: int = 3, name: str = TRAIN_WORKLOAD, opts=None, max_iter: int = 400,
                log=print):
     """(early iterate, converged iterate) pairs in the fixed frame, float32
-    numpy [nz][ny][nx], plus the in-FOV mask of the geometry."""
+    numpy [n][nz'][ny][nx] over the interior slices, plus the in-plane loss
+    mask (object support) of the geometry."""
     import ctbb_icd_b200 as CB
 
     opts = opts or CB.icd_opts(mode=CB.ICD_GROUPED, weights=CB.SSM_FP32)
@@ -245,13 +282,30 @@ def make_pairs(ctx, seeds, n_early: int = 3, name: str = TRAIN_WORKLOAD, opts=No
         x_early = scan.rc.volume()
         n = converge(scan, opts, max_iter=max_iter)
         xc = scan.rc.volume()
-        xs.append(to_fixed(ctx, scan, x_early))
-        xcs.append(to_fixed(ctx, scan, xc))
-        mask = scan.fov_mask
+        sl = interior(xc.shape[0])
+        xs.append(to_fixed(ctx, scan, x_early)[sl])
+        xcs.append(to_fixed(ctx, scan, xc)[sl])
+        mask = scan.obj_mask
         log(f"seed {s}: converged after {n + n_early} iterations, early->converged "
-            f"{rmse_hu(x_early, xc, scan.fov_mask):.1f} HU ({time.time() - t0:.1f} s)")
+            f"{scan.error_hu(x_early, xc):.1f} HU ({time.time() - t0:.1f} s)")
         scan.rc.free()
     return np.stack(xs), np.stack(xcs), mask
+
+
+def tuned_opts(ctx, name: str = TRAIN_WORKLOAD, n_early: int = 3, seed: int = 0, log=print):
+    """Autotuned grouped-ICD options for a geometry, probed after n_early
+    iterations of a seeded scan."""
+    import ctbb_icd_b200 as CB
+
+    scan = make_scan(ctx, name, seed)
+    base = CB.icd_opts(mode=CB.ICD_GROUPED, weights=CB.SSM_FP32)
+    scan.rc.iterate(scan.ssm, n_early, base)
+    best, trials = scan.rc.autotune(scan.ssm, base, probe_iters=2)
+    if log:
+        log(f"autotune {name}: warps {best.warps_in_flight}, tile {best.lattice} "
+            f"({len(trials)} trials)")
+    scan.rc.free()
+    return best, trials
 
 
 def train(net: WarmStartNet, x_early: np.ndarray, x_conv: np.ndarray, mask2d: np.ndarray, steps: int = 1500,
@@ -321,7 +375,7 @@ def time_to_tolerance(scan: Scan, x_ref: np.ndarray, opts, tol_hu: float = 0.5, 
                       net: WarmStartNet | None = None, n_early: int = 3, prio_fraction: float = 0.2,
                       prio_passes: int = 2, refresh_every: int = 10):
     """Iterate from the zero start until RMSE(x, x_ref) <= tol_hu inside the
-    FOV. With `net`, after n_early plain iterations the warm start is applied
+    object support on the interior slices (Scan.error_hu). With `net`, after n_early plain iterations the warm start is applied
     and `prio_passes` passes over the top `prio_fraction` voxels run before
     plain iterations resume. Returns the wall time of the reconstruction work
     (RMSE checks excluded), the full iterations run and the trace."""
@@ -333,8 +387,7 @@ def time_to_tolerance(scan: Scan, x_ref: np.ndarray, opts, tol_hu: float = 0.5, 
     it = 0
 
     def check_done(label):
-        x = scan.rc.volume()
-        e = rmse_hu(x, x_ref, scan.fov_mask)
+        e = scan.error_hu(scan.rc.volume(), x_ref)
         trace.append((label, elapsed, e))
         return e <= tol_hu
 

@@ -4,10 +4,11 @@
         [--steps 1500] [--out ctbb_icd_b200/weights/warm_start.npz] [--report report.json]
 
 1. For each seed: synthetic scan of the training geometry (cfg2's scanner,
-   flying focal spot, penalty and 0.6 mm voxels, 512 x 512 x 8), n_early
+   flying focal spot, penalty and 0.6 mm voxels, 512 x 512 x 16), n_early
    plain grouped-ICD iterations from the zero start (the network's input),
    then plain ICD to a relative cost change below 1e-7 per iteration (the
-   target); both rotated to the fixed frame.
+   target); both rotated to the fixed frame, interior slices kept. Grouped
+   ICD runs with autotuned warps in flight and tile edge.
 2. Adam on random crops (8 x 128 x 128) of the training pairs.
 3. Held-out seeds: loss before and after training, and time to <= 0.5 HU
    RMSE against the plain converged image for plain ICD and for the learned
@@ -54,9 +55,11 @@ def main(argv=None):
 
     torch.cuda.set_device(0)
     ctx = C.Context(0)
-    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
     report = {"args": vars(args), "workload": L.TRAIN_WORKLOAD}
     log = lambda m: print(m, flush=True)  # noqa: E731
+    opts, trials = L.tuned_opts(ctx, n_early=args.n_early, log=log)
+    report["autotune"] = trials
+    report["opts"] = {"warps_in_flight": opts.warps_in_flight, "lattice": opts.lattice}
 
     t0 = time.time()
     if args.pairs and os.path.exists(args.pairs):

@@ -208,6 +208,13 @@ def phantom_spec(name_or_dict):
     return spec
 
 
+def slab_clip(rp, slice_locations) -> tuple:
+    """z range (cm) covered by the reconstructed slices: the phantom clip that
+    makes the synthetic data consistent with the slab being reconstructed."""
+    half = 0.5 * float(rp.geom.voxel_size_z)
+    return float(min(slice_locations)) - half, float(max(slice_locations)) + half
+
+
 def materialise(name: str, directory: str, *, raw: bool = True, n_threads: int | None = None,
                 overrides: dict | None = None):
     """Write <directory>/<name>.prm (and the synthetic raw file) for a workload.

@@ -188,6 +188,8 @@ typedef struct ctbb_phantom_spec {
     double ellipsoid_z_hi;
     double i0_lo;          /* incident photons per ray; <= 0 -> noise free  */
     double i0_hi;          /* > i0_lo -> drawn per view in [i0_lo, i0_hi]   */
+    double clip_z_lo;      /* clip_z_hi > clip_z_lo: every object is cut to  */
+    double clip_z_hi;      /* this z range (cm), a phantom of finite length  */
 } ctbb_phantom_spec;
 
 /* CPU projector: writes raw[Readings][n_channels][Nrows_projection]. */
@@ -273,7 +275,9 @@ typedef struct ctbb_icd_opts {
     double relax;             /* grouped: step scale omega in (0, 2) (0: 1.0)     */
     int32_t priority;         /* grouped: visit only the priority subset built by
                                  ctbb_gpu_recon_set_priority (0: every voxel)     */
-    int32_t reserved2;
+    int32_t warps_per_voxel;  /* grouped: 1 (0), 4 or 8 warps per voxel update; with
+                                 4 or 8 the update's matrix entries stay in registers
+                                 between gather and scatter                       */
 } ctbb_icd_opts;
 
 typedef struct ctbb_iter_stats {
@@ -387,17 +391,21 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
 
 /*
  * Autotuner for grouped ICD (no reference counterpart). From the current
- * iterate, runs probe_iters iterations for each candidate pair (warps in
- * flight, tile edge of the visiting order) and keeps the pair with the
+ * iterate, runs probe_iters iterations for each candidate (warps per voxel,
+ * warps in flight, tile edge of the visiting order) and keeps the one with the
  * largest decrease of the FP64 cost per millisecond of device time. The
- * iterate and e are restored afterwards; *best = *base with the two fields
- * set. Candidates: 1, 2, 4, ..., 32 times the coupling-bound default of
- * warps (at most 48 per SM) and tile edges nx/16, nx/8, nx/4.
+ * iterate and e are restored afterwards; *best = *base with the three fields
+ * set. Candidates: one warp per voxel at 1, 2, 4, ..., 32 times the
+ * coupling-bound default of warps in flight (at most 48 per SM); 8 warps per
+ * voxel with 1 or 2 updates per SM; 4 warps per voxel with 2 or 4 per SM;
+ * each with tile edges nx/16, nx/8, nx/4.
  */
 #define CTBB_TUNE_MAX_TRIALS 32
 typedef struct ctbb_tune_trial {
     int32_t warps_in_flight;
+    int32_t warps_per_voxel;
     int32_t lattice;
+    int32_t reserved;
     double device_ms;   /* ICD kernel time of the probe iterations */
     double cost;        /* FP64 cost after them                    */
     double score;       /* (start_cost - cost) / device_ms         */

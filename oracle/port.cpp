@@ -409,7 +409,7 @@ extern "C" void port_synth(const ctbb_geom_c* g, const ctbb_phantom_spec* spec, 
         for (int64_t c = 0; c < nch; ++c)
             for (int64_t r = 0; r < nr; ++r) {
                 const uint64_t ray = (uint64_t)((v * nch + c) * nr + r);
-                const double p = ctbb_line_integral(G, objs.data(), (int)objs.size(), v, c, r);
+                const double p = ctbb_line_integral(G, objs.data(), (int)objs.size(), v, c, r, spec->clip_z_lo, spec->clip_z_hi);
                 raw[ray] = ctbb_noisy_sample(p, i0, spec->seed, ray);
             }
     }

@@ -183,3 +183,53 @@ def test_warm_start_applies_rotated_correction(ctx):
     # leaves those voxels out.
     assert 0 < st.voxel_updates < x0.size
     net.free()
+
+
+def test_autotune_leaves_iterate_and_picks_a_candidate(ctx):
+    scan = L.make_scan(ctx, "cfg1_small", seed=2)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
+    scan.rc.iterate(scan.ssm, 2, opts)
+    scan.rc.refresh_residual(scan.ssm)
+    x0, c0 = scan.rc.volume(), scan.rc.cost()
+    best, trials = scan.rc.autotune(scan.ssm, opts, probe_iters=1)
+    assert np.array_equal(scan.rc.volume(), x0)
+    assert abs(scan.rc.cost() - c0) <= 1e-12 * abs(c0)
+    chosen = [t for t in trials if t["best"]]
+    assert len(chosen) == 1 and chosen[0]["score"] == max(t["score"] for t in trials)
+    assert (best.warps_in_flight, best.warps_per_voxel, best.lattice) == (
+        chosen[0]["warps_in_flight"], chosen[0]["warps_per_voxel"], chosen[0]["lattice"])
+    assert {t["warps_per_voxel"] for t in trials} == {1, 4, 8}
+    st = scan.rc.iterate(scan.ssm, 2, best)
+    assert st.iterations == 2
+
+
+def test_trained_warm_start_beats_plain_icd(ctx):
+    """The committed network on a scan it was not trained on (seed 905 of the
+    training geometry): after the warm start and the same number of full
+    iterations, the FP64 cost is below plain ICD's after twice as many
+    iterations, and the image is closer to a longer plain run's."""
+    net = L.WarmStartNet.load(ctx)
+    scan = L.make_scan(ctx, L.TRAIN_WORKLOAD, seed=905)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
+    n = 12
+
+    scan.rc.iterate(scan.ssm, 2 * n, opts)
+    scan.rc.refresh_residual(scan.ssm)
+    c_plain_2n = scan.rc.cost()
+    x_plain_2n = scan.rc.volume()
+    scan.rc.iterate(scan.ssm, 6 * n, opts)
+    x_long = scan.rc.volume()
+
+    scan.rc.set_volume(scan.ssm, None)
+    scan.rc.iterate(scan.ssm, 3, opts)
+    scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
+    popts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, priority=True)
+    scan.rc.set_priority(0.2, popts)
+    scan.rc.iterate(scan.ssm, 2, popts)
+    scan.rc.iterate(scan.ssm, n - 3, opts)
+    scan.rc.refresh_residual(scan.ssm)
+    c_learned = scan.rc.cost()
+    x_learned = scan.rc.volume()
+    assert c_learned < c_plain_2n, (c_learned, c_plain_2n)
+    assert scan.error_hu(x_learned, x_long) < scan.error_hu(x_plain_2n, x_long)
+    net.free()

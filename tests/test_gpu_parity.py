@@ -196,15 +196,15 @@ def converged_cfg1_small(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights", [C.SSM_FP32, C.SSM_FP16])
-def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights):
+@pytest.mark.parametrize("weights,wpv", [(C.SSM_FP32, 1), (C.SSM_FP16, 1), (C.SSM_FP32, 8), (C.SSM_FP16, 4)])
+def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv):
     rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
     rc = C.Recon(rp, data.slice_indices, ctx)
     rc.set_raw(data.raw)
     rc.set_volume(ssm, None)
     costs = []
     for _ in range(6):
-        rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5))
+        rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5, warps_per_voxel=wpv))
         rc.refresh_residual(ssm)
         costs.append(rc.cost())
     x = rc.volume_f64()
