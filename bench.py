@@ -169,7 +169,11 @@ def run_ours(args, rank, world, dist):
         rc.iterate(ssm, 3, opts)
         opts, trials = rc.autotune(ssm, opts, probe_iters=2)
         tune = {"chosen": {"warps_per_voxel": opts.warps_per_voxel, "warps_in_flight": opts.warps_in_flight,
-                           "lattice": opts.lattice}, "trials": len(trials)}
+                           "lattice": opts.lattice},
+                "trials": [[t["warps_per_voxel"], t["warps_in_flight"], t["lattice"], round(t["device_ms"], 1),
+                            round(t["score"], 1)] for t in trials],
+                "trial_fields": ["warps_per_voxel", "warps_in_flight", "lattice", "ms_2_iterations",
+                                 "cost_decrease_per_ms"]}
         rc.set_volume(ssm, None)
 
     # Algorithmic bytes per iteration (one launch): e read + written once per

@@ -91,6 +91,7 @@ struct ctbb_recon {
     float* d_prio = nullptr;
     uint32_t* d_prio_order = nullptr;
     uint64_t n_prio_order = 0;
+    int prio_P = 0;
 };
 
 struct ctbb_cnn;
@@ -119,6 +120,9 @@ ctbb_status launch_icd_sequential(ctbb_recon* rc, const ctbb_ssm* ssm, int n_ite
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o,
                                float* ms, double* entries, uint64_t* items);
 int default_warps_in_flight(const ctbb_recon* rc);
+int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o);
+uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o);
+uint64_t max_items_in_flight(uint64_t n_items, int nz, int T);
 ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out);
 
 // rotate.cu

@@ -472,6 +472,25 @@ __global__ void order_keys_kernel(OrderParams O, const double* __restrict__ cs, 
     }
 }
 
+// Rotated voxel centres snapped to the fixed grid can land two (rarely three)
+// in-plane neighbours of one slice on the same cell: equal keys, adjacent in
+// the sorted order, so they would be updated concurrently although they share
+// nearly all of their rays. Every occupant after the first moves to a
+// sub-phase after its cell's rank (key = rank * M + rest becomes
+// (2 rank + 1) * M + rest, M = Q * n_tiles * nz), a whole rank sweep away.
+__global__ void split_collisions_kernel(const uint64_t* __restrict__ sorted, uint64_t n, uint64_t M,
+                                        uint64_t* __restrict__ keys_out) {
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t k = sorted[p];
+        if (k == ~0ull) {
+            keys_out[p] = k;
+            continue;
+        }
+        const uint64_t dup = (p > 0 && sorted[p - 1] == k) ? 1ull : 0ull;
+        keys_out[p] = (2ull * (k / M) + dup) * M + k % M;
+    }
+}
+
 // Sum of in-range entries over (column inside the FOV, slice): the unit of
 // work of one iteration. One warp per column.
 __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uint32_t* __restrict__ vptr,
@@ -523,14 +542,50 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     return P;
 }
 
-// Tile edge T (cells): 8 tiles per axis by default (longer raster sweeps
-// converge faster per iteration, measured on the 512 x 512 x 64 workload);
-// `lattice` overrides it.
+}  // namespace
+
+namespace ctbb {
+
+// Concurrency bound of the visiting order. Items are sorted by (cell rank in
+// tile, slice parity, tile, slice): the items of one cell rank (about n / T^2,
+// both parities) lie a whole tile apart in-plane; the next rank holds their
+// in-plane neighbours, which share nearly all of their rays. With at most one
+// rank's worth of updates in flight, no two in-plane neighbours of a slice
+// are updated together. Adjacent slices of one cell (the two parities of a
+// rank) may be: they overlap in about half of their detector rows, and
+// updating them together keeps their sinogram sectors in L2 once.
+uint64_t max_items_in_flight(uint64_t n_items, int nz, int T) {
+    (void)nz;
+    return std::max<uint64_t>(1, n_items / ((uint64_t)T * (uint64_t)T));
+}
+
+// Voxel updates the options ask to keep in flight (warps_in_flight counts
+// warps; an update takes warps_per_voxel of them).
+uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o) {
+    const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
+    const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
+    return std::max<uint64_t>(1, (uint64_t)(W / wpv));
+}
+
+// Tile edge T (cells); `lattice` overrides it. Default: the largest power of
+// two up to nx/4 whose cell ranks hold at least the requested in-flight
+// updates (longer raster sweeps converge faster per iteration, measured on
+// the 512 x 512 x 64 workload).
 int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     const int nx = (int)rc->geom.num_voxels_x;
-    const int P = o.lattice > 0 ? o.lattice : std::max(4, nx / 8);
-    return std::max(1, std::min(P, nx));
+    if (o.lattice > 0) return std::max(1, std::min(o.lattice, nx));
+    const uint64_t items = requested_items(rc, o);
+    const int nz = (int)rc->geom.num_voxels_z;
+    int T = 4;
+    while (2 * T <= std::max(4, nx / 4) && max_items_in_flight(rc->nvox, nz, 2 * T) >= items) T *= 2;
+    return std::min(T, nx);
 }
+
+}  // namespace ctbb
+
+namespace {
+
+using namespace ctbb;
 
 // Visiting order for tile edge P_lat, optionally restricted to the voxels
 // whose priority is at least thr.
@@ -596,6 +651,15 @@ ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float
     if (e == cudaSuccess) e = cudaMalloc(&d_tmp, tmp_bytes);
     if (e == cudaSuccess)
         e = cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_k0, d_k1, d_v0, d_v1, (int)n, 0, 64, st);
+    if (e == cudaSuccess) {
+        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
+        const uint64_t M = (uint64_t)O.Q * O.n_tiles * (uint64_t)O.nz;
+        split_collisions_kernel<<<grid, 256, 0, st>>>(d_k1, n, M, d_k0);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(d_tmp, tmp_bytes, d_k0, d_k1, d_v1, d_v0, (int)n, 0, 64, st);
+    if (e == cudaSuccess) std::swap(d_v0, d_v1);  // sorted values back in d_v1
     // Items outside the FOV sort last with key ~0; count the valid prefix.
     uint64_t n_valid = n;
     if (e == cudaSuccess) {
@@ -678,7 +742,8 @@ int default_warps_in_flight(const ctbb_recon* rc) {
 
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
                                double* entries, uint64_t* items) {
-    CTBB_TRY(build_order(rc, lattice_spacing(rc, o)));
+    const int T = lattice_spacing(rc, o);
+    CTBB_TRY(build_order(rc, T));
     if (o.priority && !rc->d_prio_order)
         return fail(CTBB_ERR_INVALID_ARG, "priority pass requested but no priority set (ctbb_gpu_recon_set_priority)");
     const bool prio = o.priority != 0;
@@ -686,12 +751,14 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     if (prio) P.n_items = rc->n_prio_order;
     const uint32_t* order = prio ? rc->d_prio_order : rc->d_order;
     if (items) *items = P.n_items;
+    // Updates in flight: as requested, within the order's concurrency bound.
+    const uint64_t in_flight = std::min<uint64_t>(
+        requested_items(rc, o), max_items_in_flight(P.n_items, P.nz, prio ? rc->prio_P : T));
     if (entries) {
         CTBB_TRY(inrange_entries(rc, ssm, entries));
         // A priority pass visits a subset; scale by the share of items.
         if (prio && rc->n_order > 0) *entries *= (double)rc->n_prio_order / (double)rc->n_order;
     }
-    const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
     const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     if (wpv != 1 && wpv != 4 && wpv != 8)
         return fail(CTBB_ERR_INVALID_ARG, "warps_per_voxel must be 1, 4 or 8 (got %d)", wpv);
@@ -708,7 +775,7 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
     if (wpv == 1) {
-        const int blocks = std::max(1, (W + 7) / 8);
+        const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
         if (h)
             icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
                                                                rc->d_e32, rc->d_x32, ctx->d_queue);
@@ -716,8 +783,7 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
             icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
                                                               rc->d_e32, rc->d_x32, ctx->d_queue);
     } else {
-        // warps_in_flight counts warps: W / wpv voxel updates in flight.
-        const int blocks = std::max(1, W / wpv);
+        const int blocks = (int)in_flight;
         if (wpv == 8) {
             if (h)
                 icd_cta_kernel<__half, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
@@ -899,6 +965,16 @@ extern "C" ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* b, const ctbb_icd_opts
     if (wsel != CTBB_SSM_FP16 && wsel != CTBB_SSM_FP32) return fail(CTBB_ERR_INVALID_ARG, "weights must be FP16 or FP32");
     double entries = 0.0;
     int nx_max = 1;
+    double n_sum = 0.0;
+    for (ctbb_recon* rc : b->recons) {
+        n_sum += (double)rc->nvox;
+        nx_max = std::max(nx_max, (int)rc->geom.num_voxels_x);
+    }
+    // Each scan gets a share of the in-flight items proportional to its size,
+    // so the per-scan coupling bound uses the whole batch's item count.
+    int warps = o.warps_in_flight > 0
+                    ? o.warps_in_flight
+                    : std::max(4, std::min(b->ctx->sm_count * 32, (int)(0.4 * n_sum / (3.2 * nx_max))));
     bool orders_changed = b->d_merged == nullptr || b->merged_T.size() != b->recons.size();
     std::vector<int> T(b->recons.size());
     for (size_t i = 0; i < b->recons.size(); ++i) {
@@ -907,12 +983,14 @@ extern "C" ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* b, const ctbb_icd_opts
         if ((wsel == CTBB_SSM_FP16 && !s->d_w16) || (wsel == CTBB_SSM_FP32 && !s->d_w32))
             return fail(CTBB_ERR_INVALID_ARG, "scan %zu: matrix does not hold the requested weights", i);
         CTBB_TRY(recon_to_grouped(rc, s));
-        T[i] = lattice_spacing(rc, o);
+        ctbb_icd_opts oi = o;
+        oi.warps_per_voxel = 1;
+        oi.warps_in_flight = std::max(1, (int)((double)warps * (double)rc->nvox / n_sum));
+        T[i] = lattice_spacing(rc, oi);
         CTBB_TRY(build_order(rc, T[i]));
         double en = 0.0;
         CTBB_TRY(inrange_entries(rc, s, &en));
         entries += en;
-        nx_max = std::max(nx_max, (int)rc->geom.num_voxels_x);
         if (!orders_changed && b->merged_T[i] != T[i]) orders_changed = true;
     }
     if (orders_changed) {
@@ -921,11 +999,14 @@ extern "C" ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* b, const ctbb_icd_opts
         drop_graph(b);
     }
     const double relax = (o.relax > 0.0 && o.relax < 2.0) ? o.relax : 1.0;
-    // Each scan gets a share of the in-flight items proportional to its size,
-    // so the per-scan coupling bound uses the whole batch's item count.
-    const int warps = o.warps_in_flight > 0
-                          ? o.warps_in_flight
-                          : std::max(4, std::min(b->ctx->sm_count * 32, (int)(0.4 * (double)b->n_total / (3.2 * nx_max))));
+    // Within every scan's order concurrency bound (its share of the items).
+    for (size_t i = 0; i < b->recons.size(); ++i) {
+        const ctbb_recon* rc = b->recons[i];
+        if (rc->n_order == 0) continue;
+        const double cap = (double)max_items_in_flight(rc->n_order, (int)rc->geom.num_voxels_z, T[i]) *
+                           (double)b->n_total / (double)rc->n_order;
+        warps = std::max(1, std::min(warps, (int)cap));
+    }
     if (!b->graph || b->graph_warps != warps || b->graph_relax != relax || b->graph_weights != wsel) {
         if (wsel == CTBB_SSM_FP16) {
             CTBB_TRY(upload_scans<__half>(b, o));
@@ -1003,9 +1084,11 @@ extern "C" ctbb_status ctbb_gpu_recon_set_priority(ctbb_recon* rc, const ctbb_ic
     if (e != cudaSuccess) return fail(CTBB_ERR_CUDA, "priority threshold: %s", cudaGetErrorString(e));
     uint32_t* order = nullptr;
     uint64_t n_order = 0;
-    CTBB_TRY(build_order_into(rc, lattice_spacing(rc, o), rc->d_prio, thr, &order, &n_order));
+    const int T = lattice_spacing(rc, o);
+    CTBB_TRY(build_order_into(rc, T, rc->d_prio, thr, &order, &n_order));
     cudaFree(rc->d_prio_order);
     rc->d_prio_order = order;
     rc->n_prio_order = n_order;
+    rc->prio_P = T;
     return CTBB_OK;
 }

@@ -47,10 +47,12 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     ctbb_status status = CTBB_OK;
     if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
 
-    // Candidates (warps per voxel, warps in flight): one warp per voxel at
-    // multiples of the coupling-bound default; 8 warps per voxel with one or
-    // two updates per SM; 4 warps per voxel with two or four per SM. Tile
-    // edges of 1/16, 1/8 and 1/4 of the slice.
+    // Candidates (warps per voxel, warps in flight, tile edge): one warp per
+    // voxel at multiples of the coupling-bound default; 8 warps per voxel with
+    // one or two updates per SM; 4 warps per voxel with two or four per SM;
+    // each with the default tile edge for that concurrency and half of it.
+    // Launches cap the updates in flight at the visiting order's bound, so
+    // candidates that collapse onto the same effective shape run once.
     const int w0 = default_warps_in_flight(rc);
     const int sms = rc->ctx->sm_count;
     const int wmax = sms * 48;
@@ -61,31 +63,34 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     }
     for (int per_sm : {1, 2}) ws.push_back({8, 8 * sms * per_sm});
     for (int per_sm : {2, 4}) ws.push_back({4, 4 * sms * per_sm});
-    const int nx = (int)rc->geom.num_voxels_x;
-    std::vector<int> ts;
-    for (int d : {16, 8, 4}) {
-        const int t = std::max(4, nx / d);
-        if (std::find(ts.begin(), ts.end(), t) == ts.end()) ts.push_back(t);
-    }
     struct Trial {
         int wpv, w, t;
         double ms, cost, score;
     };
     std::vector<Trial> trials;
     int ibest = -1;
-    for (int t : ts) {
-        for (const auto& pw : ws) {
-            const int wpv = pw.first, w = pw.second;
-            if (status != CTBB_OK) break;
-            if (trials.size() >= CTBB_TUNE_MAX_TRIALS) break;
+    for (const auto& pw : ws) {
+        for (int half = 0; half < 2; ++half) {
+            if (status != CTBB_OK || trials.size() >= CTBB_TUNE_MAX_TRIALS) break;
+            ctbb_icd_opts c = o;
+            c.warps_in_flight = pw.second;
+            c.warps_per_voxel = pw.first;
+            c.lattice = 0;
+            const int t_auto = lattice_spacing(rc, c);
+            c.lattice = half ? std::max(4, t_auto / 2) : t_auto;
+            if (half && c.lattice == t_auto) continue;
+            const uint64_t items = std::min<uint64_t>(
+                requested_items(rc, c), max_items_in_flight(rc->n_order ? rc->n_order : rc->nvox,
+                                                            (int)rc->geom.num_voxels_z, c.lattice));
+            c.warps_in_flight = (int)(items * (uint64_t)pw.first);
+            bool seen = false;
+            for (const Trial& tr : trials)
+                seen |= tr.wpv == c.warps_per_voxel && tr.w == c.warps_in_flight && tr.t == c.lattice;
+            if (seen) continue;
             if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
                 status = fail(CTBB_ERR_CUDA, "autotune restore");
                 break;
             }
-            ctbb_icd_opts c = o;
-            c.warps_in_flight = w;
-            c.warps_per_voxel = wpv;
-            c.lattice = t;
             double ms_tot = 0.0;
             for (int i = 0; i < probe_iters && status == CTBB_OK; ++i) {
                 float ms = 0.f;
@@ -98,7 +103,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             if (status == CTBB_OK) status = cost_f64(rc, ssm, false, &cost);
             if (status != CTBB_OK) break;
             const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
-            trials.push_back({wpv, w, t, ms_tot, cost, score});
+            trials.push_back({c.warps_per_voxel, c.warps_in_flight, c.lattice, ms_tot, cost, score});
             if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
         }
     }

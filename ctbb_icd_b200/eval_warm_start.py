@@ -62,7 +62,7 @@ def main(argv=None):
     # Reference: learned start, then ref_iter iterations with FP64 refreshes.
     t0 = time.time()
     scan.rc.set_volume(scan.ssm, None)
-    scan.rc.iterate(scan.ssm, args.n_early, opts)
+    scan.rc.iterate(scan.ssm, args.n_early, net.early_opts(scan.rc, opts))
     scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
     done = 0
     prev = None
@@ -89,9 +89,24 @@ def main(argv=None):
                                   prio_passes=args.prio_passes)
     log(f"learned: {learned['seconds']:.2f} s, {learned['iterations']} iterations, reached {learned['reached']}")
 
+    ladder = [1000.0, 500.0, 200.0, 100.0, 50.0, 25.0, 10.0, 5.0, 1.0, args.tol]
+
+    def seconds_to(r, tol):
+        for _, t, e in r["trace"]:
+            if e <= tol:
+                return t
+        return None
+
+    thresholds = []
+    for tol in ladder:
+        a, b = seconds_to(plain, tol), seconds_to(learned, tol)
+        thresholds.append({"hu": tol, "plain_s": a, "learned_s": b,
+                           "ratio": (b / a) if (a is not None and b is not None and a > 0) else None})
+
     def brief(r):
         tr = r["trace"]
         pick = tr[:6] + [t for t in tr[6:] if t[0].startswith("iter") and int(t[0].split()[1]) % 25 == 0] + tr[-1:]
+        # (label, seconds, HU) at the start, every 25 iterations and the end
         return {"seconds": r["seconds"], "iterations": r["iterations"], "reached": r["reached"],
                 "final_hu": tr[-1][2], "trace": [(a, round(s, 3), round(e, 3)) for a, s, e in pick]}
 
@@ -106,6 +121,7 @@ def main(argv=None):
         "plain": brief(plain), "learned": brief(learned),
         "ratio_learned_over_plain": (learned["seconds"] / plain["seconds"]
                                      if plain["reached"] and learned["reached"] else None),
+        "time_to_threshold": thresholds,
         "error_region": "object support r < 13 cm, interior slices",
     }
     line = json.dumps(out, default=float)

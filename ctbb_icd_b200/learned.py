@@ -111,9 +111,26 @@ class WarmStartNet:
         check(lib().ctbb_cnn_adam_step(self.handle, float(lr), float(beta1), float(beta2), float(eps),
                                        float(grad_scale)))
 
+    # The network's input is the iterate after `n_early` grouped iterations
+    # run with a fixed visiting-order tile edge and a fixed density of
+    # concurrent updates (in-flight updates per voxel): the protocol its
+    # training pairs were made with. early_opts() reproduces it on any volume.
+    n_early = 3
+    early_lattice = 32
+    early_density = 2048.0 / (512 * 512 * 16)
+
+    def early_opts(self, rc, base):
+        import ctbb_icd_b200 as CB
+
+        nvox = int(np.prod(rc.rp.shape))
+        return CB.icd_opts(mode=base.mode, weights=base.weights, lattice=self.early_lattice,
+                           warps_in_flight=max(32, int(round(self.early_density * nvox))))
+
     def save(self, path: str, **meta):
         s_in, s_out = self.scaling()
         os.makedirs(os.path.dirname(os.path.abspath(path)), exist_ok=True)
+        meta = dict(dict(n_early=self.n_early, early_lattice=self.early_lattice,
+                         early_density=self.early_density), **meta)
         np.savez(path, params=self.params(), blocks=self.blocks, s_in=s_in, s_out=s_out,
                  **{k: np.asarray(v) for k, v in meta.items()})
 
@@ -123,6 +140,11 @@ class WarmStartNet:
         net = cls(ctx, int(d["blocks"]))
         net.set_params(d["params"])
         net.set_scaling(float(d["s_in"]), float(d["s_out"]))
+        for k in ("n_early", "early_lattice"):
+            if k in d:
+                setattr(net, k, int(d[k]))
+        if "early_density" in d:
+            net.early_density = float(d["early_density"])
         return net
 
     def free(self):
@@ -264,7 +286,7 @@ def converge(scan: Scan, opts, max_iter: int = 400, rel: float = 1e-7, refresh_e
 
 
 def make_pairs(ctx, seeds, n_early: int = 3, name: str = TRAIN_WORKLOAD, opts=None, max_iter: int = 400,
-               log=print):
+               log=print, early_opts=None):
     """(early iterate, converged iterate) pairs in the fixed frame, float32
     numpy [n][nz'][ny][nx] over the interior slices, plus the in-plane loss
     mask (object support) of the geometry."""
@@ -278,7 +300,7 @@ def make_pairs(ctx, seeds, n_early: int = 3, name: str = TRAIN_WORKLOAD, opts=No
         t0 = time.time()
         scan = make_scan(ctx, name, s, ssm)
         ssm = scan.ssm
-        scan.rc.iterate(ssm, n_early, opts)
+        scan.rc.iterate(ssm, n_early, early_opts(scan.rc) if early_opts else opts)
         x_early = scan.rc.volume()
         n = converge(scan, opts, max_iter=max_iter)
         xc = scan.rc.volume()
@@ -392,7 +414,8 @@ def time_to_tolerance(scan: Scan, x_ref: np.ndarray, opts, tol_hu: float = 0.5, 
         return e <= tol_hu
 
     if net is not None:
-        _, dt = _timed(lambda: scan.rc.iterate(scan.ssm, n_early, opts))
+        eopts = net.early_opts(scan.rc, opts)
+        _, dt = _timed(lambda: scan.rc.iterate(scan.ssm, n_early, eopts))
         elapsed += dt
         it += n_early
         check_done(f"plain x{n_early}")

@@ -61,20 +61,29 @@ def main(argv=None):
     report["autotune"] = trials
     report["opts"] = {"warps_in_flight": opts.warps_in_flight, "lattice": opts.lattice}
 
+    # The early-iterate protocol the network is trained for (and recorded
+    # with its weights): the tuned tile edge and density of in-flight updates.
+    net = L.WarmStartNet(ctx, args.blocks, seed=0)
+    nvox = int(np.prod(L.make_scan(ctx, L.TRAIN_WORKLOAD, 0, clip=False).rp.shape))
+    net.n_early = args.n_early
+    net.early_lattice = int(opts.lattice)
+    net.early_density = float(opts.warps_in_flight) / max(1, opts.warps_per_voxel) / nvox
     t0 = time.time()
     if args.pairs and os.path.exists(args.pairs):
         z = np.load(args.pairs)
         xe, xc, he, hc, mask = z["xe"], z["xc"], z["he"], z["hc"], z["mask"]
     else:
+        def early(rc):
+            return net.early_opts(rc, opts)
+
         xe, xc, mask = L.make_pairs(ctx, _seeds(args.train_seeds), n_early=args.n_early, opts=opts,
-                                    max_iter=args.max_iter, log=log)
+                                    max_iter=args.max_iter, log=log, early_opts=early)
         he, hc, _ = L.make_pairs(ctx, _seeds(args.heldout_seeds), n_early=args.n_early, opts=opts,
-                                 max_iter=args.max_iter, log=log)
+                                 max_iter=args.max_iter, log=log, early_opts=early)
         if args.pairs:
             np.savez(args.pairs, xe=xe, xc=xc, he=he, hc=hc, mask=mask)
     report["data_seconds"] = time.time() - t0
 
-    net = L.WarmStartNet(ctx, args.blocks, seed=0)
     report["heldout_loss_init"] = L.eval_loss(net, he, hc, mask)
     t0 = time.time()
     hist = L.train(net, xe, xc, mask, steps=args.steps, batch=args.batch, lr=args.lr, log=log)

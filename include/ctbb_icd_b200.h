@@ -268,8 +268,10 @@ typedef struct ctbb_icd_opts {
     int32_t mode;             /* CTBB_ICD_*                                       */
     int32_t weights;          /* grouped mode: CTBB_SSM_FP32 or CTBB_SSM_FP16     */
     int32_t refresh_every;    /* grouped: FP64 y - Ax refresh every K iterations (0: never) */
-    int32_t warps_in_flight;  /* grouped: concurrent voxel updates (0: autotune)  */
-    int32_t lattice;          /* grouped: in-plane spacing of the visiting order (0: auto) */
+    int32_t warps_in_flight;  /* grouped: warps kept busy (0: coupling-bound default);
+                                 capped at one cell rank of the visiting order      */
+    int32_t lattice;          /* grouped: tile edge of the visiting order (0: derived from
+                                 the warps in flight)                              */
     int32_t compute_cost;     /* evaluate the FP64 cost after each iteration      */
     double stop_rel_change;   /* stop when |dcost|/cost < this (0: fixed count)   */
     double relax;             /* grouped: step scale omega in (0, 2) (0: 1.0)     */
@@ -398,7 +400,11 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
  * set. Candidates: one warp per voxel at 1, 2, 4, ..., 32 times the
  * coupling-bound default of warps in flight (at most 48 per SM); 8 warps per
  * voxel with 1 or 2 updates per SM; 4 warps per voxel with 2 or 4 per SM;
- * each with tile edges nx/16, nx/8, nx/4.
+ * each with the default tile edge for that concurrency and half of it.
+ * Every launch keeps at most one cell rank of the visiting order (about
+ * n / T^2 updates for tile edge T) in flight, so no two in-plane neighbours
+ * of a slice are ever updated together; trials report the effective warps
+ * in flight.
  */
 #define CTBB_TUNE_MAX_TRIALS 32
 typedef struct ctbb_tune_trial {

@@ -221,7 +221,7 @@ def test_trained_warm_start_beats_plain_icd(ctx):
     x_long = scan.rc.volume()
 
     scan.rc.set_volume(scan.ssm, None)
-    scan.rc.iterate(scan.ssm, 3, opts)
+    scan.rc.iterate(scan.ssm, net.n_early, net.early_opts(scan.rc, opts))
     scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
     popts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, priority=True)
     scan.rc.set_priority(0.2, popts)
