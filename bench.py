@@ -216,7 +216,8 @@ def run_ours(args, rank, world, dist):
         peak, peak_kind = measured_peak()
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
-        traffic = read_traffic()
+        kernel = "icd_grouped_kernel" if opts.warps_per_voxel <= 1 else "icd_cta_kernel"
+        traffic = read_traffic(kernel)
         out = {
             "metric": "voxel-updates/s",
             "value": value,
@@ -244,7 +245,7 @@ def run_ours(args, rank, world, dist):
             "roofline": {
                 "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": achieved / peak, "traffic": traffic,
-                "kernel": "icd_grouped_kernel" if opts.warps_per_voxel <= 1 else "icd_cta_kernel",
+                "kernel": kernel,
                 "algorithmic_bytes_per_launch": b_iter,
                 "kernel_ms_per_launch": kernel_ms_per_launch, "peak_source": peak_kind,
             },
@@ -304,9 +305,10 @@ def run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, torch, torch_stream):
             "launches": launches_per * args.e2e_steps}
 
 
-def read_traffic():
-    """DRAM bytes per launch of icd_grouped_kernel from the committed ncu summary."""
-    p = os.path.join(ROOT, "profiles", "icd_grouped_cfg2.md")
+def read_traffic(kernel: str = "icd_grouped_kernel"):
+    """DRAM bytes per launch of the ICD kernel from the committed ncu summary
+    of that kernel on this workload."""
+    p = os.path.join(ROOT, "profiles", f"{kernel.replace('_kernel', '')}_cfg2.md")
     if not os.path.exists(p):
         return None
     for line in open(p):
@@ -481,8 +483,9 @@ def main():
     ap.add_argument("--warps", type=int, default=0, help="warps in flight (0: auto)")
     ap.add_argument("--lattice", type=int, default=0)
     ap.add_argument("--wpv", type=int, default=1, help="warps per voxel update: 1, 4 or 8")
-    ap.add_argument("--autotune", action="store_true", help="pick warps per voxel, warps in flight and tile "
-                    "edge with the library's autotuner before timing")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="skip the library's autotuner (warps per voxel, warps in flight, tile edge) and use "
+                         "--wpv/--warps/--lattice as given")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=2)
     ap.add_argument("--e2e-iters", type=int, default=10, help="ICD iterations per drop-in call")

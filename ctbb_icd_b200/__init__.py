@@ -252,7 +252,7 @@ class Ssm:
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
              compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False,
-             warps_per_voxel=1) -> IcdOpts:
+             warps_per_voxel=1, entries_per_lane=0) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
@@ -260,6 +260,7 @@ def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_fligh
     o.relax = float(relax)
     o.priority = int(bool(priority))
     o.warps_per_voxel = int(warps_per_voxel)
+    o.entries_per_lane = int(entries_per_lane)
     return o
 
 
@@ -334,7 +335,7 @@ class Recon:
         check(lib().ctbb_gpu_recon_autotune(self.handle, ssm.handle, C.byref(opts or icd_opts()),
                                             int(probe_iters), C.byref(best), C.byref(rep)))
         trials = [dict(warps_in_flight=t.warps_in_flight, warps_per_voxel=t.warps_per_voxel,
-                       lattice=t.lattice, device_ms=t.device_ms,
+                       entries_per_lane=t.entries_per_lane, lattice=t.lattice, device_ms=t.device_ms,
                        cost=t.cost, score=t.score, best=(i == rep.best))
                   for i, t in enumerate(rep.trials[:rep.n_trials])]
         return best, trials

@@ -99,12 +99,12 @@ class IcdOpts(C.Structure):
     _fields_ = [
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
-        ("priority", _I), ("warps_per_voxel", _I),
+        ("priority", _I), ("warps_per_voxel", _I), ("entries_per_lane", _I), ("reserved3", _I),
     ]
 
 
 class TuneTrial(C.Structure):
-    _fields_ = [("warps_in_flight", _I), ("warps_per_voxel", _I), ("lattice", _I), ("reserved", _I),
+    _fields_ = [("warps_in_flight", _I), ("warps_per_voxel", _I), ("lattice", _I), ("entries_per_lane", _I),
                 ("device_ms", _D), ("cost", _D), ("score", _D)]
 
 

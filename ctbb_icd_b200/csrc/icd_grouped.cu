@@ -92,17 +92,50 @@ __device__ __forceinline__ float ldw<__half>(const __half* w, int64_t m) {
     return __half2float(__ldg(w + m));
 }
 
+// L2 eviction policies: a voxel update reads its matrix entries twice (gather,
+// then scatter); the gather's loads ask L2 to keep the lines, the scatter's
+// to drop them first.
+__device__ __forceinline__ uint64_t l2_keep() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ uint64_t l2_drop() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+__device__ __forceinline__ int ld_idx(const int32_t* p, uint64_t pol) {
+    int v;
+    asm volatile("ld.global.nc.L2::cache_hint.b32 %0, [%1], %2;" : "=r"(v) : "l"(p), "l"(pol));
+    return v;
+}
+template <class WT>
+__device__ __forceinline__ float ldw_hint(const WT* w, int64_t m, uint64_t pol);
+template <>
+__device__ __forceinline__ float ldw_hint<float>(const float* w, int64_t m, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.nc.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(w + m), "l"(pol));
+    return v;
+}
+template <>
+__device__ __forceinline__ float ldw_hint<__half>(const __half* w, int64_t m, uint64_t pol) {
+    unsigned short v;
+    asm volatile("ld.global.nc.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(w + m), "l"(pol));
+    return __half2float(__ushort_as_half(v));
+}
+
 // Entries m, m+32, ..., m+32(U-1) of a column: sinogram index (q + off, or
 // -1 past the end) and weight (0 past the end).
 template <int U, class WT>
 __device__ __forceinline__ void load_chunk(const int32_t* __restrict__ idx, const WT* __restrict__ w, int64_t m,
-                                           int64_t en, int off, int* q, float* wt) {
+                                           int64_t en, int off, uint64_t pol, int* q, float* wt) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
         const int64_t mu = m + 32 * u;
         if (mu < en) {
-            q[u] = __ldg(idx + mu) + off;
-            wt[u] = ldw(w, mu);
+            q[u] = ld_idx(idx + mu, pol) + off;
+            wt[u] = ldw_hint(w, mu, pol);
         } else {
             q[u] = -1;
             wt[u] = 0.f;
@@ -110,29 +143,29 @@ __device__ __forceinline__ void load_chunk(const int32_t* __restrict__ idx, cons
     }
 }
 
-constexpr int kU = 8;      // entries per lane in flight per chunk
+constexpr int kU = 8;       // entries per lane in flight per chunk (default)
 constexpr int kStack = 16;  // same-parity slices that sweep the sinogram together
 
 // Gather beta += a e and alpha += a^2 over entries [b, en) of a column: chunks
-// of 32 x kU entries, the next chunk's indices and weights fetched while this
+// of 32 x U entries, the next chunk's indices and weights fetched while this
 // chunk's e gathers are in flight (one DRAM round trip per chunk).
-template <class WT>
+template <class WT, int U>
 __device__ __forceinline__ void gather_range(const int32_t* __restrict__ idx, const WT* __restrict__ w,
                                              const float* e, int64_t b, int64_t en, int off, int lane,
-                                             float& acc_b, float& acc_a) {
+                                             uint64_t pol, float& acc_b, float& acc_a) {
     if (b >= en) return;
-    int qa[kU];
-    float wa[kU];
-    load_chunk<kU>(idx, w, b + lane, en, off, qa, wa);
-    for (int64_t base = b; base < en; base += 32 * kU) {
-        float ev[kU];
+    int qa[U];
+    float wa[U];
+    load_chunk<U>(idx, w, b + lane, en, off, pol, qa, wa);
+    for (int64_t base = b; base < en; base += 32 * U) {
+        float ev[U];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) ev[u] = (qa[u] >= 0) ? __ldcg(e + qa[u]) : 0.f;
-        int qb[kU];
-        float wb[kU];
-        load_chunk<kU>(idx, w, base + 32 * kU + lane, en, off, qb, wb);
+        for (int u = 0; u < U; ++u) ev[u] = (qa[u] >= 0) ? __ldcg(e + qa[u]) : 0.f;
+        int qb[U];
+        float wb[U];
+        load_chunk<U>(idx, w, base + 32 * U + lane, en, off, pol, qb, wb);
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < U; ++u) {
             acc_b = fmaf(wa[u], ev[u], acc_b);
             acc_a = fmaf(wa[u], wa[u], acc_a);
             qa[u] = qb[u];
@@ -141,17 +174,17 @@ __device__ __forceinline__ void gather_range(const int32_t* __restrict__ idx, co
     }
 }
 
-// e -= du * a over entries [b, en): kU independent index/weight loads per
-// lane per chunk, then kU fire-and-forget L2 reductions.
-template <class WT>
+// e -= du * a over entries [b, en): U independent index/weight loads per
+// lane per chunk, then U fire-and-forget L2 reductions.
+template <class WT, int U>
 __device__ __forceinline__ void scatter_range(const int32_t* __restrict__ idx, const WT* __restrict__ w, float* e,
-                                              int64_t b, int64_t en, int off, int lane, float du) {
-    for (int64_t base = b; base < en; base += 32 * kU) {
-        int qs[kU];
-        float ws[kU];
-        load_chunk<kU>(idx, w, base + lane, en, off, qs, ws);
+                                              int64_t b, int64_t en, int off, int lane, uint64_t pol, float du) {
+    for (int64_t base = b; base < en; base += 32 * U) {
+        int qs[U];
+        float ws[U];
+        load_chunk<U>(idx, w, base + lane, en, off, pol, qs, ws);
 #pragma unroll
-        for (int u = 0; u < kU; ++u)
+        for (int u = 0; u < U; ++u)
             if (qs[u] >= 0) atomicAdd(e + qs[u], -du * ws[u]);
     }
 }
@@ -227,7 +260,7 @@ __device__ __forceinline__ double penalty_step(const GParams& P, const float* x,
 }
 
 // One voxel update (work item `item` of a scan's visiting order) by one warp.
-template <class WT>
+template <class WT, int U = kU>
 __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* __restrict__ order,
                                              const int64_t* __restrict__ colptr, const uint32_t* __restrict__ vptr,
                                              const int32_t* __restrict__ idx, const WT* __restrict__ w,
@@ -259,8 +292,9 @@ __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* _
     // beta = sum a e, alpha = sum a^2 (FP32 accumulation per lane) over
     // [mid, en) then [b, mid).
     float acc_b = 0.f, acc_a = 0.f;
-    gather_range(idx, w, e, mid, en, off, lane, acc_b, acc_a);
-    gather_range(idx, w, e, b, mid, off, lane, acc_b, acc_a);
+    const uint64_t keep = l2_keep();
+    gather_range<WT, U>(idx, w, e, mid, en, off, lane, keep, acc_b, acc_a);
+    gather_range<WT, U>(idx, w, e, b, mid, off, lane, keep, acc_b, acc_a);
     const double beta = (double)warp_sum(acc_b);
     const double alpha = (double)warp_sum(acc_a);
 
@@ -270,12 +304,13 @@ __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* _
     if (lane == 0) x[q] = (float)(xq + upd);
     const float du = (float)upd;
     if (du != 0.f) {
-        scatter_range(idx, w, e, mid, en, off, lane, du);
-        scatter_range(idx, w, e, b, mid, off, lane, du);
+        const uint64_t drop = l2_drop();
+        scatter_range<WT, U>(idx, w, e, mid, en, off, lane, drop, du);
+        scatter_range<WT, U>(idx, w, e, b, mid, off, lane, drop, du);
     }
 }
 
-template <class WT>
+template <class WT, int U>
 __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint32_t* __restrict__ order,
                                                           const int64_t* __restrict__ colptr,
                                                           const uint32_t* __restrict__ vptr,
@@ -288,7 +323,7 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
         if (lane == 0) item = atomicAdd(queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= P.n_items) break;
-        process_item(P, order, colptr, vptr, idx, w, start, e, x, item, lane);
+        process_item<WT, U>(P, order, colptr, vptr, idx, w, start, e, x, item, lane);
     }
 }
 
@@ -774,14 +809,25 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const int64_t* cp = ssm->d_colptr;
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
+    const int epl = o.entries_per_lane > 0 ? o.entries_per_lane : kU;
+    if (epl != 8 && epl != 16) return fail(CTBB_ERR_INVALID_ARG, "entries_per_lane must be 8 or 16 (got %d)", epl);
     if (wpv == 1) {
         const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
-        if (h)
-            icd_grouped_kernel<__half><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                               rc->d_e32, rc->d_x32, ctx->d_queue);
-        else
-            icd_grouped_kernel<float><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                              rc->d_e32, rc->d_x32, ctx->d_queue);
+        if (epl == 16) {
+            if (h)
+                icd_grouped_kernel<__half, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                       rc->d_e32, rc->d_x32, ctx->d_queue);
+            else
+                icd_grouped_kernel<float, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+        } else {
+            if (h)
+                icd_grouped_kernel<__half, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+            else
+                icd_grouped_kernel<float, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+        }
     } else {
         const int blocks = (int)in_flight;
         if (wpv == 8) {

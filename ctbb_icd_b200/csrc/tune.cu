@@ -47,45 +47,52 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     ctbb_status status = CTBB_OK;
     if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
 
-    // Candidates (warps per voxel, warps in flight, tile edge): one warp per
-    // voxel at multiples of the coupling-bound default; 8 warps per voxel with
-    // one or two updates per SM; 4 warps per voxel with two or four per SM;
-    // each with the default tile edge for that concurrency and half of it.
-    // Launches cap the updates in flight at the visiting order's bound, so
-    // candidates that collapse onto the same effective shape run once.
+    // Candidates (warps per voxel, warps in flight, entries per lane, tile
+    // edge): one warp per voxel at 1/4 .. 2 times the coupling-bound default,
+    // 8 or 16 entries per lane in flight, the default tile edge for that
+    // concurrency (and half of it at the default); 4 warps per voxel with
+    // four updates per SM. Launches cap the updates in flight at the visiting
+    // order's bound, so candidates that collapse onto the same effective
+    // shape run once.
     const int w0 = default_warps_in_flight(rc);
     const int sms = rc->ctx->sm_count;
     const int wmax = sms * 48;
-    std::vector<std::pair<int, int>> ws;
-    for (int m : {1, 2, 4, 8, 16, 32}) {
-        const int w = std::max(32, std::min(wmax, w0 * m));
-        if (std::find(ws.begin(), ws.end(), std::make_pair(1, w)) == ws.end()) ws.push_back({1, w});
-    }
-    for (int per_sm : {1, 2}) ws.push_back({8, 8 * sms * per_sm});
-    for (int per_sm : {2, 4}) ws.push_back({4, 4 * sms * per_sm});
+    struct Cand {
+        int wpv, w, epl, half;
+    };
+    std::vector<Cand> cands;
+    for (int epl : {8, 16})
+        for (int m4 : {1, 2, 4, 8}) {
+            const int w = std::max(32, std::min(wmax, w0 * m4 / 4));
+            cands.push_back({1, w, epl, 0});
+            if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1});
+        }
+    cands.push_back({4, 4 * sms * 4, 8, 0});
     struct Trial {
-        int wpv, w, t;
+        int wpv, w, epl, t;
         double ms, cost, score;
     };
     std::vector<Trial> trials;
     int ibest = -1;
-    for (const auto& pw : ws) {
-        for (int half = 0; half < 2; ++half) {
+    for (const Cand& cd : cands) {
+        {
             if (status != CTBB_OK || trials.size() >= CTBB_TUNE_MAX_TRIALS) break;
             ctbb_icd_opts c = o;
-            c.warps_in_flight = pw.second;
-            c.warps_per_voxel = pw.first;
+            c.warps_in_flight = cd.w;
+            c.warps_per_voxel = cd.wpv;
+            c.entries_per_lane = cd.epl;
             c.lattice = 0;
             const int t_auto = lattice_spacing(rc, c);
-            c.lattice = half ? std::max(4, t_auto / 2) : t_auto;
-            if (half && c.lattice == t_auto) continue;
+            c.lattice = cd.half ? std::max(4, t_auto / 2) : t_auto;
+            if (cd.half && c.lattice == t_auto) continue;
             const uint64_t items = std::min<uint64_t>(
                 requested_items(rc, c), max_items_in_flight(rc->n_order ? rc->n_order : rc->nvox,
                                                             (int)rc->geom.num_voxels_z, c.lattice));
-            c.warps_in_flight = (int)(items * (uint64_t)pw.first);
+            c.warps_in_flight = (int)(items * (uint64_t)cd.wpv);
             bool seen = false;
             for (const Trial& tr : trials)
-                seen |= tr.wpv == c.warps_per_voxel && tr.w == c.warps_in_flight && tr.t == c.lattice;
+                seen |= tr.wpv == c.warps_per_voxel && tr.w == c.warps_in_flight && tr.t == c.lattice &&
+                        tr.epl == c.entries_per_lane;
             if (seen) continue;
             if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
                 status = fail(CTBB_ERR_CUDA, "autotune restore");
@@ -103,7 +110,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             if (status == CTBB_OK) status = cost_f64(rc, ssm, false, &cost);
             if (status != CTBB_OK) break;
             const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
-            trials.push_back({c.warps_per_voxel, c.warps_in_flight, c.lattice, ms_tot, cost, score});
+            trials.push_back({c.warps_per_voxel, c.warps_in_flight, c.entries_per_lane, c.lattice, ms_tot, cost, score});
             if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
         }
     }
@@ -117,6 +124,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     *best = o;
     best->warps_in_flight = trials[ibest].w;
     best->warps_per_voxel = trials[ibest].wpv;
+    best->entries_per_lane = trials[ibest].epl;
     best->lattice = trials[ibest].t;
     if (report) {
         memset(report, 0, sizeof(*report));
@@ -126,6 +134,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
         for (size_t i = 0; i < trials.size(); ++i) {
             report->trials[i].warps_in_flight = trials[i].w;
             report->trials[i].warps_per_voxel = trials[i].wpv;
+            report->trials[i].entries_per_lane = trials[i].epl;
             report->trials[i].lattice = trials[i].t;
             report->trials[i].device_ms = trials[i].ms;
             report->trials[i].cost = trials[i].cost;

@@ -206,6 +206,16 @@ def fov_mask(rp) -> np.ndarray:
     return (xx * xx + yy * yy) < (g.acquisition_fov / 2.0) ** 2
 
 
+def workload_shape(name: str):
+    """(nz, ny, nx) of a workload's reconstruction (host-side setup only)."""
+    import ctbb_icd_b200 as CB
+
+    w = W.workload(name)
+    d = tempfile.mkdtemp(prefix="ctbb_shape_")
+    w["prm"].update(sinogram_path=os.path.join(d, "raw.bin"), output_dir=d, output_file="out.img")
+    return tuple(CB.configure_recon_params(W.write_prm(os.path.join(d, "s.prm"), w["prm"])).shape)
+
+
 def make_scan(ctx, name: str, seed: int, ssm=None, weights=None, clip: bool = True) -> Scan:
     """A workload's geometry with phantom seed `seed`: raw data from the GPU
     projector (phantom cut to the reconstructed slab unless clip=False), zero

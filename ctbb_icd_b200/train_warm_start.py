@@ -64,7 +64,7 @@ def main(argv=None):
     # The early-iterate protocol the network is trained for (and recorded
     # with its weights): the tuned tile edge and density of in-flight updates.
     net = L.WarmStartNet(ctx, args.blocks, seed=0)
-    nvox = int(np.prod(L.make_scan(ctx, L.TRAIN_WORKLOAD, 0, clip=False).rp.shape))
+    nvox = int(np.prod(L.workload_shape(L.TRAIN_WORKLOAD)))
     net.n_early = args.n_early
     net.early_lattice = int(opts.lattice)
     net.early_density = float(opts.warps_in_flight) / max(1, opts.warps_per_voxel) / nvox

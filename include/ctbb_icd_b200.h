@@ -280,6 +280,9 @@ typedef struct ctbb_icd_opts {
     int32_t warps_per_voxel;  /* grouped: 1 (0), 4 or 8 warps per voxel update; with
                                  4 or 8 the update's matrix entries stay in registers
                                  between gather and scatter                       */
+    int32_t entries_per_lane; /* grouped, one warp per voxel: matrix entries each lane
+                                 keeps in flight per round trip, 8 (0) or 16      */
+    int32_t reserved3;
 } ctbb_icd_opts;
 
 typedef struct ctbb_iter_stats {
@@ -394,13 +397,14 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
 /*
  * Autotuner for grouped ICD (no reference counterpart). From the current
  * iterate, runs probe_iters iterations for each candidate (warps per voxel,
- * warps in flight, tile edge of the visiting order) and keeps the one with the
+ * warps in flight, entries per lane, tile edge of the visiting order) and
+ * keeps the one with the
  * largest decrease of the FP64 cost per millisecond of device time. The
- * iterate and e are restored afterwards; *best = *base with the three fields
- * set. Candidates: one warp per voxel at 1, 2, 4, ..., 32 times the
- * coupling-bound default of warps in flight (at most 48 per SM); 8 warps per
- * voxel with 1 or 2 updates per SM; 4 warps per voxel with 2 or 4 per SM;
- * each with the default tile edge for that concurrency and half of it.
+ * iterate and e are restored afterwards; *best = *base with the four fields
+ * set. Candidates: one warp per voxel at 1/4, 1/2, 1 and 2 times the
+ * coupling-bound default of warps in flight, with 8 or 16 entries per lane
+ * in flight and the default tile edge for that concurrency (half of it too
+ * at the default); 4 warps per voxel with four updates per SM.
  * Every launch keeps at most one cell rank of the visiting order (about
  * n / T^2 updates for tile edge T) in flight, so no two in-plane neighbours
  * of a slice are ever updated together; trials report the effective warps
@@ -411,7 +415,7 @@ typedef struct ctbb_tune_trial {
     int32_t warps_in_flight;
     int32_t warps_per_voxel;
     int32_t lattice;
-    int32_t reserved;
+    int32_t entries_per_lane;
     double device_ms;   /* ICD kernel time of the probe iterations */
     double cost;        /* FP64 cost after them                    */
     double score;       /* (start_cost - cost) / device_ms         */
