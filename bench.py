@@ -161,7 +161,7 @@ def run_ours(args, rank, world, dist):
     setup_s = time.time() - t0
     info = ssm.info()
     opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice,
-                      warps_per_voxel=args.wpv)
+                      warps_per_voxel=args.wpv, entries_per_lane=args.epl)
     nvox = int(np.prod(rp.shape))
     tune = None
     if args.autotune:
@@ -169,11 +169,11 @@ def run_ours(args, rank, world, dist):
         rc.iterate(ssm, 3, opts)
         opts, trials = rc.autotune(ssm, opts, probe_iters=2)
         tune = {"chosen": {"warps_per_voxel": opts.warps_per_voxel, "warps_in_flight": opts.warps_in_flight,
-                           "lattice": opts.lattice},
-                "trials": [[t["warps_per_voxel"], t["warps_in_flight"], t["lattice"], round(t["device_ms"], 1),
-                            round(t["score"], 1)] for t in trials],
-                "trial_fields": ["warps_per_voxel", "warps_in_flight", "lattice", "ms_2_iterations",
-                                 "cost_decrease_per_ms"]}
+                           "entries_per_lane": opts.entries_per_lane, "lattice": opts.lattice},
+                "trials": [[t["warps_per_voxel"], t["warps_in_flight"], t["entries_per_lane"], t["lattice"],
+                            round(t["device_ms"], 1), round(t["score"], 1)] for t in trials],
+                "trial_fields": ["warps_per_voxel", "warps_in_flight", "entries_per_lane", "lattice",
+                                 "ms_2_iterations", "cost_decrease_per_ms"]}
         rc.set_volume(ssm, None)
 
     # Algorithmic bytes per iteration (one launch): e read + written once per
@@ -237,6 +237,7 @@ def run_ours(args, rank, world, dist):
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
                 "warps_in_flight": opts.warps_in_flight or "auto", "warps_per_voxel": max(1, opts.warps_per_voxel),
+                "entries_per_lane": opts.entries_per_lane or 8,
                 "lattice": opts.lattice or "auto", "autotune": tune,
                 "l2": "inputs larger than L2 (e 1.74 GB, SSM > 20 GB)",
                 "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
@@ -483,6 +484,7 @@ def main():
     ap.add_argument("--warps", type=int, default=0, help="warps in flight (0: auto)")
     ap.add_argument("--lattice", type=int, default=0)
     ap.add_argument("--wpv", type=int, default=1, help="warps per voxel update: 1, 4 or 8")
+    ap.add_argument("--epl", type=int, default=0, help="entries per lane in flight: 8 or 16 (0: 8)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="skip the library's autotuner (warps per voxel, warps in flight, tile edge) and use "
                          "--wpv/--warps/--lattice as given")
