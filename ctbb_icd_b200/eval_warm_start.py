@@ -65,7 +65,6 @@ def main(argv=None):
     scan.rc.iterate(scan.ssm, args.n_early, net.early_opts(scan.rc, opts))
     scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
     done = 0
-    prev = None
     while done < args.ref_iter:
         n = min(50, args.ref_iter - done)
         scan.rc.iterate(scan.ssm, n, opts)
