@@ -161,7 +161,7 @@ def run_ours(args, rank, world, dist):
     setup_s = time.time() - t0
     info = ssm.info()
     opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice,
-                      warps_per_voxel=args.wpv, entries_per_lane=args.epl)
+                      warps_per_voxel=args.wpv, entries_per_lane=args.epl, stage_column=max(0, args.stage_column))
     nvox = int(np.prod(rp.shape))
     tune = None
     if args.autotune:
@@ -176,13 +176,12 @@ def run_ours(args, rank, world, dist):
                                  "ms_2_iterations", "cost_decrease_per_ms"]}
         rc.set_volume(ssm, None)
 
-    # Algorithmic bytes per iteration (one launch): e read + written once per
-    # in-range entry (8 B), the SSM read once (index + weight), image r+w.
     rc.iterate(ssm, args.warmup, opts)
-    st = rc.iterate(ssm, 1, opts)  # also yields the in-range entry count
+    st = rc.iterate(ssm, 1, opts)
     entries = rc.entries(ssm)
     w_bytes = 2 if weights_fmt == C.SSM_FP16 else 4
-    b_iter = 8.0 * entries + (4 + w_bytes) * float(info.nnz) + 8.0 * nvox
+    # The iterate the timed region starts from, for the e2e leg (same range).
+    x_start = rc.volume() if args.e2e else None
 
     clocks = ClockSampler(local, enabled=args.clocks)
     if dist:
@@ -200,10 +199,18 @@ def run_ours(args, rank, world, dist):
     elapsed_ms = start.elapsed_time(end)
     clocks.stop()
     kernel_ms_per_launch = st.device_ms / max(1, st.iterations)
+    # Algorithmic bytes per iteration (one launch), from what the timed
+    # launches did: e read once per in-range entry gathered (4 B) and written
+    # once per entry of the updates that changed their voxel (4 B; an update
+    # with du == 0, e.g. an air voxel held at 0 by the positivity clamp,
+    # scatters nothing), the matrix read once (index + weight), image r+w.
+    gathered = st.entries / max(1, st.iterations)
+    scattered = st.entries_scattered / max(1, st.iterations)
+    b_iter = 4.0 * gathered + 4.0 * scattered + (4 + w_bytes) * float(info.nnz) + 8.0 * nvox
 
     e2e = None
     if args.e2e:
-        e2e = run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, torch, torch_stream)
+        e2e = run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, x_start)
 
     from ctbb_icd_b200.replicas import max_over_ranks
 
@@ -216,7 +223,8 @@ def run_ours(args, rank, world, dist):
         peak, peak_kind = measured_peak()
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
-        kernel = "icd_grouped_kernel" if opts.warps_per_voxel <= 1 else "icd_cta_kernel"
+        kernel = ("icd_staged_kernel" if opts.stage_column else "icd_grouped_kernel") \
+            if opts.warps_per_voxel <= 1 else "icd_cta_kernel"
         traffic = read_traffic(kernel)
         out = {
             "metric": "voxel-updates/s",
@@ -236,6 +244,7 @@ def run_ours(args, rank, world, dist):
                 "weights": args.weights, "error_sinogram": "fp32", "voxels": nvox,
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
+                "scattered_entries_per_iter": scattered, "stage_column": int(opts.stage_column),
                 "warps_in_flight": opts.warps_in_flight or "auto", "warps_per_voxel": max(1, opts.warps_per_voxel),
                 "entries_per_lane": opts.entries_per_lane or 8,
                 "lattice": opts.lattice or "auto", "autotune": tune,
@@ -258,7 +267,7 @@ def run_ours(args, rank, world, dist):
                           "h2d_bytes_per_step": e2e["h2d"], "d2h_bytes_per_step": e2e["d2h"]}
             out["gpu_launches"] += e2e["launches"]
         if args.cpu_baseline and world == 1:
-            cb = cpu_sample(ctx, iterations=3)
+            cb = cpu_sample(iterations=3)
             out["cpu_baseline"] = {k: cb.get(k) for k in ("value", "unit", "cores", "kind", "sample")}
     rc.free()
     ssm.free()
@@ -266,43 +275,199 @@ def run_ours(args, rank, world, dist):
     return out
 
 
-def run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, torch, torch_stream):
+def _geometry(workdir, name):
+    """The workload's recon params and slice tables (no raw data)."""
+    import ctbb_icd_b200 as C
+    from ctbb_icd_b200 import workloads as W
+
+    prm = W.workload(name)["prm"]
+    prm.update(sinogram_path=os.path.join(workdir, "raw.bin"), output_dir=workdir, output_file="out.img")
+    open(prm["sinogram_path"], "wb").close()
+    rp = C.configure_recon_params(W.write_prm(os.path.join(workdir, "stage.prm"), prm))
+    return rp, C.slice_tables(rp)
+
+
+def run_stage(args):
+    """--stage ssm | rotate: the other two subsystems of the path on their own.
+
+    ssm: generate_system_matrix_ffs on the GPU (cell-count pass, column scan,
+    fill pass), FP16 weights, timed per build; algorithmic bytes = the matrix
+    written (index + weight per entry, per-view offsets, column pointers).
+    rotate: rotate_slices_rotating2fixed of the workload's volume, device to
+    device; algorithmic bytes = the volume read once and written once."""
+    import torch
+
+    import ctbb_icd_b200 as C
+
+    torch.cuda.set_device(0)
+    ctx = C.Context(0)
+    workdir = tempfile.mkdtemp(prefix="ctbb_stage_")
+    peak, peak_kind = measured_peak()
+    clocks = ClockSampler(0, enabled=args.clocks)
+    if args.stage == "cnn":
+        line = _stage_cnn(args, C, ctx, torch, clocks)
+        line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                     "data": "synthetic", "clocks": clocks.summary()})
+        ctx.close()
+        return line
+    rp, tables = _geometry(workdir, args.workload)
+    if args.stage == "ssm":
+        for _ in range(args.warmup):
+            C.Ssm.generate(rp, ctx, C.SSM_FP16).free()
+        clocks.start()
+        ms, info = [], None
+        for _ in range(args.steps):
+            s = C.Ssm.generate(rp, ctx, C.SSM_FP16)
+            info = s.info()
+            ms.append(info.build_ms)
+            s.free()
+        clocks.stop()
+        ncol, nvsm = int(info.n_columns), int(info.n_views)
+        out_bytes = 6.0 * info.nnz + 4.0 * ncol * (nvsm + 1) + 8.0 * (ncol + 1)
+        t = float(np.median(ms))
+        line = {"metric": "ssm-entries/s", "value": info.nnz / (t / 1e3), "unit": "entries/s",
+                "ms_per_step": t, "config": {"workload": args.workload, "stage": "generate_system_matrix",
+                                             "nnz": int(info.nnz), "columns": ncol, "views": nvsm,
+                                             "weights": "fp16"},
+                "roofline": {"bound": "hbm", "achieved": out_bytes / (t / 1e3) / 1e9, "peak": peak,
+                             "unit": "GB/s", "frac": out_bytes / (t / 1e3) / 1e9 / peak,
+                             "kernel": "ssm_cells_kernel (count + fill)", "algorithmic_bytes_per_launch": out_bytes,
+                             "peak_source": peak_kind}}
+    else:
+        nvox = int(np.prod(rp.shape))
+        vin = torch.rand(nvox, device="cuda", dtype=torch.float32)
+        vout = torch.empty_like(vin)
+        ta = np.ascontiguousarray(tables.tube_angles, np.float64)
+        si = np.ascontiguousarray(tables.slice_indices, np.uint64)
+
+        def one():
+            C.check(C.lib().ctbb_gpu_rotate_device(ctx.handle, ctypes.byref(rp.geom), C.ptr(ta, ctypes.c_double),
+                                                   C.ptr(si, ctypes.c_uint64), ctypes.c_void_p(vin.data_ptr()),
+                                                   ctypes.c_void_p(vout.data_ptr()), C.ROTATE_ROTATING2FIXED))
+
+        for _ in range(args.warmup):
+            one()
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")  # larger than L2
+        clocks.start()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            one()
+            b.record()
+            b.synchronize()
+            ms.append(a.elapsed_time(b))
+        clocks.stop()
+        t = float(np.median(ms))
+        out_bytes = 8.0 * nvox
+        line = {"metric": "voxels/s", "value": nvox / (t / 1e3), "unit": "voxels/s", "ms_per_step": t,
+                "config": {"workload": args.workload, "stage": "rotate_slices_rotating2fixed",
+                           "voxels": nvox, "l2": "256 MB buffer written between steps (L2 flushed)"},
+                "roofline": {"bound": "hbm", "achieved": out_bytes / (t / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                             "frac": out_bytes / (t / 1e3) / 1e9 / peak, "kernel": "rotate_kernel",
+                             "algorithmic_bytes_per_launch": out_bytes, "peak_source": peak_kind}}
+    line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+                 "dtype": line.get("dtype", "f32"), "data": "synthetic", "clocks": clocks.summary()})
+    ctx.close()
+    subprocess.run(["rm", "-rf", workdir])
+    return line
+
+
+def _stage_cnn(args, C, ctx, torch, clocks):
+    """--stage cnn: the warm-start network's tensor-core convolutions on a
+    --cnn-shape volume (default 16 x 256 x 256): time per forward pass and
+    per training step (forward, loss, backward, gradient accumulation), and
+    the FLOP rate of the 32 -> 32 convolutions (2 x 27 x 32 x 32 FLOP per
+    voxel each: 2 per residual block forward; forward, backward-data and
+    weight gradient per block in a training step)."""
+    import json as _json
+
+    from ctbb_icd_b200 import learned as L
+
+    shape = args.cnn_shape
+    net = L.WarmStartNet(ctx, 4, seed=0)
+    g = torch.Generator(device="cuda").manual_seed(0)
+    x = (0.15 + 0.1 * torch.rand(*shape, device="cuda", generator=g)).contiguous()
+    xc = (x + 0.002 * torch.randn(*shape, device="cuda", generator=g)).contiguous()
+    nvox = x.numel()
+    conv_flop = 2.0 * 27 * 32 * 32 * nvox
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(args.steps):
+            fn()
+        b.record()
+        b.synchronize()
+        return a.elapsed_time(b) / args.steps
+
+    clocks.start()
+    fwd_ms = timed(lambda: net.forward(x))
+    train_ms = timed(lambda: net.accumulate_gradient(x, xc))
+    clocks.stop()
+    net.zero_gradient()
+    net.free()
+    fwd_tflops = 2 * 4 * conv_flop / (fwd_ms / 1e3) / 1e12
+    peak = None
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            peak = _json.load(f).get("bf16_tflops")
+    return {"metric": "network voxels/s", "value": nvox / (fwd_ms / 1e3), "unit": "voxels/s",
+            "ms_per_step": fwd_ms, "dtype": "bf16 operands, fp32 accumulation",
+            "config": {"workload": f"warm-start CNN forward, 4 residual blocks x 32 channels, volume {shape}",
+                       "stage": "cnn", "train_step_ms": train_ms,
+                       "train_conv_tflops": 6 * 4 * conv_flop / (train_ms / 1e3) / 1e12},
+            "roofline": {"bound": "tensor", "achieved": fwd_tflops, "peak": peak, "unit": "TFLOP/s",
+                         "frac": fwd_tflops / peak if peak else None, "kernel": "conv_mid_kernel",
+                         "algorithmic_flops_per_pass": 2 * 4 * conv_flop,
+                         "peak_source": "measured" if peak else None}}
+
+
+def run_e2e(C, ctx, rp, tables, ssm, rc, opts, args, x_start):
     """The same metric through ctbb_gpu_icd (the icd_iteration drop-in) with
-    pinned host buffers: per step one call that uploads the raw data and the
-    zero initial image, runs the workload's iteration count and returns the
-    image (what a caller of icd_iteration does)."""
+    pinned host buffers, over the same iteration range as the device-timed
+    region: each call uploads the raw data and the iterate the timed region
+    started from, creates the reconstruction state (FP64 A x refresh of the
+    error sinogram included), runs `steps` iterations with the same settings
+    and returns the image."""
+    import torch
+
     raw = torch.empty(rp.raw_shape, dtype=torch.float32).pin_memory()
     C.check(C.lib().ctbb_gpu_recon_get_raw(rc.handle, C.ptr(raw.numpy(), ctypes.c_float)))
-    vol = torch.zeros(rp.shape, dtype=torch.float32).pin_memory()
+    x0 = torch.from_numpy(np.ascontiguousarray(x_start, np.float32)).pin_memory()
+    vol = torch.empty_like(x0).pin_memory()
     g = C.GeomC.from_buffer_copy(rp.geom)
-    g.num_iterations = args.e2e_iters
+    g.num_iterations = args.steps
     si = np.ascontiguousarray(tables.slice_indices, np.uint64)
     st = C.IterStats()
 
     def one():
+        vol.copy_(x0)
         C.check(C.lib().ctbb_gpu_icd(ctx.handle, ssm.handle, ctypes.byref(g), C.ptr(si, ctypes.c_uint64),
                                      C.ptr(raw.numpy(), ctypes.c_float), C.ptr(vol.numpy(), ctypes.c_float),
                                      ctypes.byref(opts), ctypes.byref(st)))
 
-    def reset():
-        vol.zero_()
-
-    reset()
     one()  # warm-up
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.e2e_steps):
-        reset()
         one()
     torch.cuda.synchronize()
     secs = time.perf_counter() - t0
     nvox = int(np.prod(rp.shape))
-    # Kernel launches per call: residual init, f64->f32 image and residual
-    # conversion (2), e2e_iters ICD iterations, entry count (first call only).
-    launches_per = 3 + args.e2e_iters
-    return {"value": nvox * args.e2e_iters * args.e2e_steps / secs, "seconds": secs,
-            "updates": nvox * args.e2e_iters * args.e2e_steps,
-            "h2d": int(raw.numel() * 4 + vol.numel() * 4), "d2h": int(vol.numel() * 4),
+    # Kernel launches per call: residual refresh (forward projection, residual),
+    # image conversion, entry count and visiting order (order keys, collision
+    # split), then one ICD launch per iteration.
+    launches_per = 6 + args.steps
+    return {"value": nvox * args.steps * args.e2e_steps / secs, "seconds": secs,
+            "updates": nvox * args.steps * args.e2e_steps,
+            "h2d": int(raw.numel() * 4 + x0.numel() * 4), "d2h": int(vol.numel() * 4),
             "launches": launches_per * args.e2e_steps}
 
 
@@ -327,146 +492,136 @@ def read_traffic(kernel: str = "icd_grouped_kernel"):
 CPU_SAMPLE = dict(nx=64, nz=16, readings=3200)
 
 
-def _sample_prm(nx, nz, readings):
-    """Benchmark geometry restricted to an nx x nx x nz central sub-volume at
-    the same voxel size, over `readings` views, with a z-range the scan covers."""
-    import ctbb_icd_b200 as C
+def _sample_inrange_entries(g, slice_indices, colptr, idx):
+    """In-range matrix entries per voxel of a sample (the icd_iteration.cpp:
+    205-207 window test), from its matrix and slice table."""
+    per_view = int(g.n_channels) * int(g.Nrows_projection)
+    limit = int(g.Readings) * per_view
+    half = int(g.num_views_for_system_matrix) // 2
+    total = 0
+    q = idx.astype(np.int64)
+    for si in slice_indices:
+        off = (int(si) - half) * per_view
+        total += int(np.count_nonzero((q + off >= 0) & (q + off < limit)))
+    return total / float(len(slice_indices) * (len(colptr) - 1))
+
+
+def reference_sample(iterations, *, own_matrix, extra_builds=(), workdir=None):
+    """Run the reference program (oracle/_ref, the CTBB_ICD sources built
+    unmodified; icd_ref_cores = -O2 with OpenMP on every host processor) on a
+    bounded sample of the benchmark workload: the same scanner, views per
+    turn, flying focal spot, voxel size, slice thickness, phantom and
+    penalty, on a 64 x 64 x 16 central sub-volume (3.75 cm FOV) over the 3200
+    views around it. Geometry comes from the reference's own setup code and
+    the raw frames from the oracle's CPU projector; no library of this
+    package is loaded.
+
+    own_matrix: the reference generates its matrix.bin itself (its
+    generate_system_matrix_ffs time is reported); otherwise the oracle's
+    builder writes it (byte-identical, tests/test_reference_run.py), which
+    keeps the sample within seconds. extra_builds: other reference builds
+    ("shipped" = -g with its hard-coded 11 threads, "O2" = -O2 with 11
+    threads) timed for 2 iterations on the same matrix."""
     from ctbb_icd_b200 import workloads as W
+    from oracle import reference_run as R
 
-    w = W.workload(WORKLOAD)
-    prm = w["prm"]
-    dx = prm["recon_fov"] / prm["nx"]
-    prm.update(nx=nx, ny=nx, recon_fov=dx * nx, Readings=readings)
-    d = tempfile.mkdtemp(prefix="ctbb_ref_")
-    prm.update(sinogram_path=os.path.join(d, "raw.bin"), output_dir=d, output_file="ref.img",
-               matrix_path=os.path.join(d, "matrix.bin"))
-    open(prm["sinogram_path"], "wb").close()
-    # Allowed window of setup.cpp:359-371 for this geometry; centre the slab in it.
-    rp = C.configure_recon_params(W.write_prm(os.path.join(d, "ref.prm"), dict(prm, z_start=-1.0, z_end=-1.1)))
-    g = rp.geom
-    tzi, vz = g.tube_z_increment, g.voxel_size_z
-    zf = (float(readings) / float(g.num_views_per_turn)) * g.table_feed_per_rotation / 10.0
-    half = np.ceil(0.5 * g.beam_width_at_roi_edge / vz) * vz
-    lo, hi = zf - (readings - 1) * tzi + half, zf - half
-    mid = 0.5 * (lo + hi)
-    z_start = mid + 0.5 * nz * vz
-    prm.update(z_start=z_start, z_end=z_start - (nz + 0.5) * vz)
-    return w, prm, d
-
-
-def cpu_sample(ctx=None, iterations=3, threads=None):
-    """Time the reference program's ICD iterations on a bounded sample of the
-    benchmark geometry: same scanner, views per turn, flying focal spot,
-    voxel size (0.586 mm) and slice thickness, but a 64 x 64 x 16 central
-    sub-volume (3.75 cm FOV) and the 3200 views around it. The matrix.bin it
-    reads is exported from the GPU builder, which reproduces the reference's
-    generate_system_matrix_ffs bit for bit (tests/test_gpu_parity.py); the
-    reference's own generator would take minutes single-threaded here.
-
-    The reference's time per voxel grows with the matrix entries it visits,
-    and the small FOV shortens the system-matrix window (num_views_for_system
-    _matrix follows the FOV radius), so the rate is also reported normalised
-    to the full workload's entries per voxel (`value`)."""
-    import ctbb_icd_b200 as C
-    from ctbb_icd_b200 import workloads as W
-
-    binary = os.path.join(ROOT, "oracle", "_ref", "icd_ref_O2")
-    if not os.path.exists(binary):
+    if not R.available():
         return {"value": None, "unit": "voxel-updates/s", "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/icd_ref_O2 is not built"}
+                "sample": "unavailable: the reference program is not built under oracle/_ref"}
     s = CPU_SAMPLE
-    w, prm, d = _sample_prm(s["nx"], s["nz"], s["readings"])
-    prm["num_iterations"] = iterations
-    prm_path = W.write_prm(os.path.join(d, "ref.prm"), prm)
-    own_ctx = ctx is None
-    if own_ctx:
-        ctx = C.Context(0)
-    rp = C.configure_recon_params(prm_path)
-    tables = C.slice_tables(rp)
-    spec = W.phantom_spec(w["phantom"])
-    spec.ellipsoid_z_lo, spec.ellipsoid_z_hi = prm["z_end"], prm["z_start"]
-    rc = C.Recon(rp, tables.slice_indices, ctx)
-    C.check(C.lib().ctbb_gpu_synth_raw(ctx.handle, ctypes.byref(rp.geom), ctypes.byref(spec),
-                                       ctypes.c_void_p(rc.raw_device_ptr())))
-    C.write_raw_file(prm["sinogram_path"], rp, rc.raw())
-    ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
-    ssm.export_reference(prm["matrix_path"])
-    nvox = s["nx"] * s["nx"] * s["nz"]
-    sample_entries = rc.entries(ssm) / nvox
-    rc.free()
-    ssm.free()
-    full_entries = workload_entries_per_voxel(ctx)
-    if own_ctx:
-        ctx.close()
+    d = workdir or tempfile.mkdtemp(prefix="ctbb_ref_")
+    w = W.workload(WORKLOAD)
+    prm = R.central_subvolume(dict(w["prm"], num_iterations=iterations), s["nx"], s["nz"], s["readings"], d)
+    prm_path = R.write_prm(os.path.join(d, "ref.prm"), prm)
+    R.write_zero_raw(prm["sinogram_path"], prm["Readings"], prm["n_channels"], prm["Nrows"])
+    fields, _, slices = R.setup_dump(prm_path)
+    g = R.geometry(fields)
+    ph = dict(w["phantom"], z_lo=min(prm["z_start"], prm["z_end"]), z_hi=max(prm["z_start"], prm["z_end"]))
+    t0 = time.perf_counter()
+    R.write_raw(prm["sinogram_path"], R.synth_raw(g, ph))
+    synth_s = time.perf_counter() - t0
+    matrix = os.path.join(d, "matrix.bin")
+    if not own_matrix:
+        R.write_matrix_bin(matrix, *R.oracle_matrix(g))
     ncpu = os.cpu_count() or 1
-    threads = threads or min(ncpu, 11)  # the reference hard-codes 11 OpenMP threads (icd_iteration.cpp:40)
-    env = dict(os.environ, OMP_THREAD_LIMIT=str(threads))
-    os.makedirs(os.path.join(d, "reconstructions"), exist_ok=True)
-    stamps = []
-    p = subprocess.Popen([binary, prm_path], cwd=d, env=env, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
-                         text=True, bufsize=1)
-    for line in p.stdout:
-        if line.startswith("Iteration #") or line.startswith("Rotating ICD slices"):
-            stamps.append(time.perf_counter())
-    p.wait()
-    subprocess.run(["rm", "-rf", d])
-    if p.returncode != 0 or len(stamps) < 2:
-        return {"value": None, "unit": "voxel-updates/s", "cores": threads, "kind": "reference",
-                "sample": f"reference run failed (exit {p.returncode})"}
-    per_iter = np.diff(stamps)
-    raw_rate = nvox / float(np.median(per_iter))
-    value = raw_rate * sample_entries / full_entries
-    return {"value": value, "unit": "voxel-updates/s", "cores": threads, "kind": "reference",
-            "sample": (f"reference icd_iteration (-O2 build of the unmodified sources, OpenMP {threads} threads "
-                       f"of {ncpu} cores) on a {s['nx']}x{s['nx']}x{s['nz']} central sub-volume of the benchmark "
-                       f"geometry, {s['readings']} views; median of {len(per_iter)} iterations "
-                       f"{float(np.median(per_iter)):.3f} s = {raw_rate:.4g} vu/s at {sample_entries:.0f} entries/voxel, "
-                       f"scaled to the workload's {full_entries:.0f} entries/voxel"),
-            "seconds_per_iteration": [float(t) for t in per_iter], "raw_rate": raw_rate,
-            "entries_per_voxel_sample": sample_entries, "entries_per_voxel_workload": full_entries}
-
-
-_FULL_ENTRIES = {}
-
-
-def workload_entries_per_voxel(ctx):
-    """In-range matrix entries per voxel of the full benchmark workload."""
-    if "v" not in _FULL_ENTRIES:
-        import ctbb_icd_b200 as C
-        from ctbb_icd_b200 import workloads as W
-
-        w = W.workload(WORKLOAD)
-        d = tempfile.mkdtemp(prefix="ctbb_ent_")
-        prm = dict(w["prm"], sinogram_path=os.path.join(d, "r.bin"), output_dir=d, output_file="o.img")
-        rp = C.configure_recon_params(W.write_prm(os.path.join(d, "w.prm"), prm))
-        tables = C.slice_tables(rp)
-        ssm = C.Ssm.generate(rp, ctx, C.SSM_FP16)
-        rc = C.Recon(rp, tables.slice_indices, ctx)
-        _FULL_ENTRIES["v"] = rc.entries(ssm) / float(np.prod(rp.shape))
-        rc.free()
-        ssm.free()
+    rc, stamps = R.run("cores", prm_path, d)
+    times = R.stage_times(stamps)
+    if rc != 0 or len(times["iteration_s"]) < iterations:
         subprocess.run(["rm", "-rf", d])
-    return _FULL_ENTRIES["v"]
+        return {"value": None, "unit": "voxel-updates/s", "cores": ncpu, "kind": "reference",
+                "sample": f"reference run failed (exit {rc}): " + " | ".join(l for _, l in stamps[-3:])}
+    m = _read_colptr_idx(matrix, int(g.num_voxels_x * g.num_voxels_y))
+    entries = _sample_inrange_entries(g, [sl[1] for sl in slices], *m)
+    extra = {}
+    for kind in extra_builds:
+        p2 = R.write_prm(os.path.join(d, f"ref_{kind}.prm"), dict(prm, num_iterations=2, matrix_path=matrix,
+                                                                   output_file=f"ref_{kind}.img"))
+        rc2, st2 = R.run(kind, p2, d)
+        extra[kind] = R.stage_times(st2)["iteration_s"] if rc2 == 0 else None
+    subprocess.run(["rm", "-rf", d])
+    nvox = s["nx"] * s["nx"] * s["nz"]
+    per_iter = np.asarray(times["iteration_s"], np.float64)
+    rate = nvox / float(np.median(per_iter))
+    desc = (f"reference icd_iteration (CTBB_ICD sources built unmodified at -O2, OpenMP on all {ncpu} host "
+            f"processors) on a {s['nx']}x{s['nx']}x{s['nz']} central sub-volume of the benchmark geometry "
+            f"(3.75 cm FOV, {s['readings']} views, same scanner, voxel size, phantom and penalty; "
+            f"{entries:.0f} in-range matrix entries per voxel vs {FULL_ENTRIES_PER_VOXEL:.0f} in the full "
+            f"workload, rate not rescaled); median of {len(per_iter)} iterations {float(np.median(per_iter)):.3f} s")
+    if times["ssm_s"] is not None:
+        desc += f"; its own generate_system_matrix_ffs took {times['ssm_s']:.1f} s (single thread)"
+    for kind, its in extra.items():
+        label = {"shipped": "as shipped (-g, 11 threads)", "O2": "-O2 with its 11 threads"}.get(kind, kind)
+        if its:
+            desc += f"; {label}: {float(np.median(its)):.3f} s per iteration = {nvox / float(np.median(its)):.4g} vu/s"
+    return {"value": rate, "unit": "voxel-updates/s", "cores": ncpu, "kind": "reference", "sample": desc,
+            "seconds_per_iteration": per_iter.tolist(), "ssm_s": times["ssm_s"], "synth_s": synth_s,
+            "entries_per_voxel_sample": entries, "extra_builds": extra}
+
+
+# In-range matrix entries per voxel of the full benchmark workload (the
+# 1.16e11 entries one iteration visits over 16,777,216 voxels, counted by the
+# grouped kernel's entry counter on the GPU).
+FULL_ENTRIES_PER_VOXEL = 116058564736 / 16777216
+
+
+def _read_colptr_idx(path, ncol):
+    buf = np.fromfile(path, np.uint8)
+    colptr = np.zeros(ncol + 1, np.int64)
+    parts = []
+    pos = 0
+    for c in range(ncol):
+        n = int(buf[pos:pos + 8].view(np.uint64)[0])
+        parts.append(buf[pos + 8:pos + 8 + 8 * n].view(np.int32)[0::2])
+        pos += 8 + 8 * n
+        colptr[c + 1] = colptr[c] + n
+    return colptr, np.concatenate(parts) if parts else np.zeros(0, np.int32)
+
+
+def cpu_sample(iterations=3):
+    """CPU baseline for the benchmark line (rank 0, N = 1): the reference's
+    ICD on the bounded sample, with the oracle-built matrix so the sample
+    stays within tens of seconds."""
+    return reference_sample(iterations, own_matrix=False)
 
 
 def run_reference(args, rank, world):
     if rank != 0:
         return None
-    r = cpu_sample(iterations=args.warmup + args.steps)
+    r = reference_sample(args.warmup + args.steps, own_matrix=True, extra_builds=("shipped", "O2"))
     if not r.get("value"):
         return {"impl": "reference", "unavailable": r.get("sample", "reference run failed")}
     times = r["seconds_per_iteration"][-args.steps:]
-    scale = r["entries_per_voxel_sample"] / r["entries_per_voxel_workload"]
     nvox = CPU_SAMPLE["nx"] ** 2 * CPU_SAMPLE["nz"]
-    v = nvox * len(times) / float(np.sum(times)) * scale
+    v = nvox * len(times) / float(np.sum(times))
     cb = dict(r, value=v)
     return {
         "impl": "reference", "metric": "voxel-updates/s", "value": v, "unit": "voxel-updates/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * float(np.mean(times)) / scale,
+        "ms_per_step": 1e3 * float(np.mean(times)),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": "reference CPU ICD, bounded sample of the grouped-ICD "
-                                                    "benchmark geometry", "sample": cb["sample"]},
+        "data": "synthetic (seeded phantom: water + 6 inserts + 40 ellipsoids, Poisson noise, oracle CPU projector)",
+        "config": {"workload": WORKLOAD_TEXT, "sample": cb["sample"], "ssm_generation_s": r["ssm_s"],
+                   "threads": r["cores"]},
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": v, "unit": "voxel-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -489,11 +644,16 @@ def main():
                     help="skip the library's autotuner (warps per voxel, warps in flight, tile edge) and use "
                          "--wpv/--warps/--lattice as given")
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
-    ap.add_argument("--e2e-steps", type=int, default=2)
-    ap.add_argument("--e2e-iters", type=int, default=10, help="ICD iterations per drop-in call")
+    ap.add_argument("--e2e-steps", type=int, default=1, help="timed drop-in calls (each runs --steps iterations)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-clocks", dest="clocks", action="store_false", help="skip nvidia-smi clock sampling")
     ap.add_argument("--own-stream", action="store_true", help="run on the library's own stream")
+    ap.add_argument("--stage", choices=["icd", "ssm", "rotate", "cnn"], default="icd",
+                    help="icd (default): the grouped-ICD benchmark; ssm / rotate: time the matrix builder or the "
+                         "slice rotation of the same workload on their own; cnn: the warm-start network")
+    ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
+    ap.add_argument("--stage-column", type=int, default=-1,
+                    help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -513,6 +673,8 @@ def main():
     try:
         if args.impl == "reference":
             out = run_reference(args, rank, world)
+        elif args.stage != "icd":
+            out = run_stage(args) if rank == 0 else None
         else:
             out = run_ours(args, rank, world, dist)
         if rank == 0 and out is not None:

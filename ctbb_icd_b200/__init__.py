@@ -252,7 +252,7 @@ class Ssm:
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
              compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False,
-             warps_per_voxel=1, entries_per_lane=0) -> IcdOpts:
+             warps_per_voxel=1, entries_per_lane=0, stage_column=0) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
@@ -261,7 +261,23 @@ def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_fligh
     o.priority = int(bool(priority))
     o.warps_per_voxel = int(warps_per_voxel)
     o.entries_per_lane = int(entries_per_lane)
+    o.stage_column = int(stage_column)
     return o
+
+
+def penalty_steps(ctx: "Context", penalty: int, lam: float, delta: float, alpha: np.ndarray, beta: np.ndarray,
+                  x9: np.ndarray) -> np.ndarray:
+    """The grouped mode's penalised one-voxel update on given inputs
+    (ctbb_gpu_penalty_steps): alpha, beta [n]; x9 [n, 9] = voxel value and
+    its 8 in-plane neighbours (NaN: outside the volume)."""
+    a = np.ascontiguousarray(alpha, np.float64)
+    b = np.ascontiguousarray(beta, np.float64)
+    x = np.ascontiguousarray(x9, np.float32).reshape(-1, 9)
+    out = np.empty(a.size, np.float64)
+    check(lib().ctbb_gpu_penalty_steps(ctx.handle, int(penalty), float(lam), float(delta), a.size,
+                                       ptr(a, C.c_double), ptr(b, C.c_double), ptr(x, C.c_float),
+                                       ptr(out, C.c_double)))
+    return out
 
 
 class Recon:
@@ -335,7 +351,8 @@ class Recon:
         check(lib().ctbb_gpu_recon_autotune(self.handle, ssm.handle, C.byref(opts or icd_opts()),
                                             int(probe_iters), C.byref(best), C.byref(rep)))
         trials = [dict(warps_in_flight=t.warps_in_flight, warps_per_voxel=t.warps_per_voxel,
-                       entries_per_lane=t.entries_per_lane, lattice=t.lattice, device_ms=t.device_ms,
+                       entries_per_lane=t.entries_per_lane, stage_column=t.stage_column, lattice=t.lattice,
+                       device_ms=t.device_ms,
                        cost=t.cost, score=t.score, best=(i == rep.best))
                   for i, t in enumerate(rep.trials[:rep.n_trials])]
         return best, trials

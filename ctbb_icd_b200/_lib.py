@@ -99,13 +99,13 @@ class IcdOpts(C.Structure):
     _fields_ = [
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
-        ("priority", _I), ("warps_per_voxel", _I), ("entries_per_lane", _I), ("reserved3", _I),
+        ("priority", _I), ("warps_per_voxel", _I), ("entries_per_lane", _I), ("stage_column", _I),
     ]
 
 
 class TuneTrial(C.Structure):
     _fields_ = [("warps_in_flight", _I), ("warps_per_voxel", _I), ("lattice", _I), ("entries_per_lane", _I),
-                ("device_ms", _D), ("cost", _D), ("score", _D)]
+                ("stage_column", _I), ("reserved", _I), ("device_ms", _D), ("cost", _D), ("score", _D)]
 
 
 class TuneReport(C.Structure):
@@ -115,7 +115,7 @@ class TuneReport(C.Structure):
 class IterStats(C.Structure):
     _fields_ = [
         ("iterations", _I), ("reserved", _I), ("cost", _D), ("rel_change", _D),
-        ("device_ms", _D), ("voxel_updates", _D), ("entries", _D),
+        ("device_ms", _D), ("voxel_updates", _D), ("entries", _D), ("entries_scattered", _D),
     ]
 
 
@@ -181,6 +181,7 @@ PROTOTYPES = {
     "ctbb_gpu_recon_warm_start": (_I, [_P, _P, _P, _PD]),
     "ctbb_gpu_recon_autotune": (_I, [_P, _P, C.POINTER(IcdOpts), _I, C.POINTER(IcdOpts), C.POINTER(TuneReport)]),
     "ctbb_gpu_recon_set_priority": (_I, [_P, C.POINTER(IcdOpts), _D]),
+    "ctbb_gpu_penalty_steps": (_I, [_P, _I, _D, _D, _U, _PD, _PD, _PF, _PD]),
 }
 
 _lib = None

@@ -84,11 +84,24 @@ def build_oracle(verbose: bool = False) -> None:
     root = os.path.dirname(HERE)
     oracle = os.path.join(root, "oracle")
     targets = ["port"]
-    ref = os.environ.get("CTBB_REFERENCE_SRC", "/root/reference/src")
-    if os.path.isdir(ref):
+    ref = reference_src()
+    if ref:
         targets.append("ref")
-    subprocess.run(["make", "-s", "-C", oracle, *targets, f"REF={ref}"], check=True,
+    subprocess.run(["make", "-s", "-C", oracle, *targets, f"REF={ref or ''}"], check=True,
                    stdout=None if verbose else subprocess.DEVNULL)
+
+
+def reference_src():
+    """The CTBB_ICD source tree (its src/ directory) the oracle builds the
+    reference program from: $CTBB_REFERENCE_SRC, else a checkout named
+    `reference` beside the repository's directory (reference/src) when one
+    is present; None when neither exists (then only the CPU restatement
+    is built)."""
+    env = os.environ.get("CTBB_REFERENCE_SRC")
+    if env:
+        return env if os.path.isdir(env) else None
+    guess = os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "src")
+    return guess if os.path.isfile(os.path.join(guess, "icd_iteration.cpp")) else None
 
 
 def main(argv=None):

@@ -118,7 +118,8 @@ ctbb_status launch_icd_sequential(ctbb_recon* rc, const ctbb_ssm* ssm, int n_ite
 
 // icd_grouped.cu
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o,
-                               float* ms, double* entries, uint64_t* items);
+                               float* ms, double* entries, uint64_t* items, double* scattered = nullptr);
+int stage_capacity(const ctbb_ctx* ctx, int nw, int wbytes);
 int default_warps_in_flight(const ctbb_recon* rc);
 int lattice_spacing(const ctbb_recon* rc, const ctbb_icd_opts& o);
 uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o);

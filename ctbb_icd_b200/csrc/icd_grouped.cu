@@ -62,7 +62,7 @@ struct GParams {
     int nx, ny, nz, nch, nr, nvsm, readings, penalty;
     int last_slice[2];  // last slice of each parity
     uint64_t n_items, nvsm1;
-    float lambda, delta;
+    double lambda, delta;
     double relax;  // step scale applied to the exact 1-D update before the positivity clamp
     double cvx, cvy, vx, vy, fov_limit;
 };
@@ -175,17 +175,96 @@ __device__ __forceinline__ void gather_range(const int32_t* __restrict__ idx, co
 }
 
 // e -= du * a over entries [b, en): U independent index/weight loads per
-// lane per chunk, then U fire-and-forget L2 reductions.
+// lane per chunk, then U fire-and-forget L2 reductions. Chunks run from the
+// end of the range back to its start: the entries gathered last are the ones
+// whose matrix lines and e sectors are likeliest to still be in L2.
 template <class WT, int U>
 __device__ __forceinline__ void scatter_range(const int32_t* __restrict__ idx, const WT* __restrict__ w, float* e,
                                               int64_t b, int64_t en, int off, int lane, uint64_t pol, float du) {
-    for (int64_t base = b; base < en; base += 32 * U) {
+    if (b >= en) return;
+    const int64_t nchunk = (en - b + 32 * U - 1) / (32 * U);
+    for (int64_t c = nchunk - 1; c >= 0; --c) {
+        const int64_t base = b + c * (32 * U);
         int qs[U];
         float ws[U];
         load_chunk<U>(idx, w, base + lane, en, off, pol, qs, ws);
 #pragma unroll
         for (int u = 0; u < U; ++u)
             if (qs[u] >= 0) atomicAdd(e + qs[u], -du * ws[u]);
+    }
+}
+
+// Raw weight bits for the shared-memory stage, and their value.
+template <class WT>
+struct WBits;
+template <>
+struct WBits<float> {
+    using T = float;
+    __device__ static __forceinline__ float load(const float* w, int64_t m, uint64_t pol) { return ldw_hint(w, m, pol); }
+    __device__ static __forceinline__ float value(float v) { return v; }
+};
+template <>
+struct WBits<__half> {
+    using T = unsigned short;
+    __device__ static __forceinline__ unsigned short load(const __half* w, int64_t m, uint64_t pol) {
+        unsigned short v;
+        asm volatile("ld.global.nc.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(v) : "l"(w + m), "l"(pol));
+        return v;
+    }
+    __device__ static __forceinline__ float value(unsigned short v) { return __half2float(__ushort_as_half(v)); }
+};
+
+// Gather over entries [m0, m1) of a column, which occupy stage positions
+// p0 + (m - m0): the entry's sinogram index (slice offset applied) and raw
+// weight go to the warp's shared-memory stage (positions below `cap`) while
+// its e value is gathered; chunks of 32 x U entries, the next chunk's matrix
+// entries fetched while this chunk's e gathers are in flight.
+template <class WT, int U>
+__device__ __forceinline__ void stage_gather(const int32_t* __restrict__ idx, const WT* __restrict__ w,
+                                             const float* e, int64_t m0, int64_t m1, int64_t p0, int off, int lane,
+                                             uint64_t pol, int32_t* sq, typename WBits<WT>::T* sw, int64_t cap,
+                                             float& acc_b, float& acc_a) {
+    using B = WBits<WT>;
+    if (m0 >= m1) return;
+    int qa[U];
+    typename B::T wa[U];
+    auto load = [&](int64_t base, int* q, typename B::T* wv) {
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t m = base + lane + 32 * u;
+            if (m < m1) {
+                q[u] = ld_idx(idx + m, pol) + off;
+                wv[u] = B::load(w, m, pol);
+            } else {
+                q[u] = -1;
+                wv[u] = typename B::T(0);
+            }
+        }
+    };
+    load(m0, qa, wa);
+    for (int64_t base = m0; base < m1; base += 32 * U) {
+        float ev[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) ev[u] = (qa[u] >= 0) ? __ldcg(e + qa[u]) : 0.f;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int64_t p = p0 + (base - m0) + lane + 32 * u;
+            if (qa[u] >= 0 && p < cap) {
+                sq[p] = qa[u];
+                sw[p] = wa[u];
+            }
+        }
+        int qb[U];
+        typename B::T wb[U];
+        load(base + 32 * U, qb, wb);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const float wf = B::value(wa[u]);
+            acc_b = fmaf(wf, ev[u], acc_b);
+            acc_a = fmaf(wf, wf, acc_a);
+            qa[u] = qb[u];
+            wa[u] = wb[u];
+        }
     }
 }
 
@@ -203,32 +282,28 @@ struct ScanRefs {
     float* x;
 };
 
-// Penalised 1-D update of voxel q by one warp (lanes 0-7 hold the 8 in-plane
-// neighbours of penalties.cpp:41-52 / 67-74). Returns the step before the
+constexpr double kInvSqrt2 = 1.0 / 1.41421356237309504880168872420969807;
+
+// Weight of neighbour lane 0-7 in the order {-nx-1, -nx, -nx+1, -1, +1,
+// nx-1, nx, nx+1} (penalties.cpp:39-59): 1 for edges, 1/sqrt(2) for corners.
+__device__ __forceinline__ double neighbour_weight(int lane) {
+    return (lane == 1 || lane == 3 || lane == 4 || lane == 6) ? 1.0 : kInvSqrt2;
+}
+
+// The penalised 1-D surrogate solve of one voxel by one warp. Lanes 0-7 hold
+// a neighbour's difference x_n - x_q and its weight (0 for a neighbour
+// outside the volume); other lanes hold zeros. Returns the step before the
 // positivity clamp; every lane gets the same value.
-__device__ __forceinline__ double penalty_step(const GParams& P, const float* x, int64_t q, double xq, double alpha,
-                                               double beta, int lane) {
-    const double r2 = 1.0 / 1.41421356237309504880168872420969807;
-    const int64_t nx = P.nx;
-    const int64_t nvox = (int64_t)P.nx * P.ny * P.nz;
-    double diff = 0.0, wn = 0.0;
-    if (lane < 8) {
-        const int64_t offs[8] = {-nx - 1, -nx, -nx + 1, -1, 1, nx - 1, nx, nx + 1};
-        const int64_t n = q + offs[lane];
-        if (n >= 0 && n < nvox) {
-            diff = (double)__ldcg(x + n) - xq;
-            wn = (lane == 1 || lane == 3 || lane == 4 || lane == 6) ? 1.0 : r2;
-        }
-    }
-    if (P.penalty == CTBB_PENALTY_QUADRATIC) {
+__device__ __forceinline__ double penalty_solve(int penalty, double lam, double del, double alpha, double beta,
+                                                double diff, double wn) {
+    if (penalty == CTBB_PENALTY_QUADRATIC) {
         // penalties.cpp:84 (the denominator always uses all 8 weights)
         const double sum = sum8(wn * diff);
-        return (beta + (double)P.lambda * sum) / (alpha + (double)P.lambda * (4.0 + 4.0 * r2));
+        return (beta + lam * sum) / (alpha + lam * (4.0 + 4.0 * kInvSqrt2));
     }
     if (alpha == 0.0) return 0.0;  // penalties.cpp:101-102
     // Root of f(d) = 2 alpha d - 2 beta + lambda sum w psi(d - diff),
     // psi(t) = t / (delta + |t|), inside the reference's bracket.
-    const double lam = (double)P.lambda, del = (double)P.delta;
     double lo = beta / alpha, hi = beta / alpha;
     {
         double dmin = (wn != 0.0) ? diff : lo, dmax = (wn != 0.0) ? diff : hi;
@@ -259,13 +334,59 @@ __device__ __forceinline__ double penalty_step(const GParams& P, const float* x,
     return c;
 }
 
+// Penalised 1-D update of voxel q by one warp (lanes 0-7 hold the 8 in-plane
+// neighbours of penalties.cpp:41-52 / 67-74, flat-index offsets, a neighbour
+// outside [0, nvox) dropped).
+__device__ __forceinline__ double penalty_step(const GParams& P, const float* x, int64_t q, double xq, double alpha,
+                                               double beta, int lane) {
+    const int64_t nx = P.nx;
+    const int64_t nvox = (int64_t)P.nx * P.ny * P.nz;
+    double diff = 0.0, wn = 0.0;
+    if (lane < 8) {
+        // Lane -> flat-index offset {-nx-1, -nx, -nx+1, -1, +1, nx-1, nx, nx+1}.
+        const int64_t dr = lane < 3 ? -1 : (lane < 5 ? 0 : 1);
+        const int64_t dc = lane < 3 ? lane - 1 : (lane < 5 ? 2 * lane - 7 : lane - 6);
+        const int64_t n = q + dr * nx + dc;
+        if (n >= 0 && n < nvox) {
+            diff = (double)__ldcg(x + n) - xq;
+            wn = neighbour_weight(lane);
+        }
+    }
+    return penalty_solve(P.penalty, P.lambda, P.delta, alpha, beta, diff, wn);
+}
+
+// One warp per voxel: the grouped update's penalty solve on given inputs
+// (ctbb_gpu_penalty_steps). x9[9 i] is the voxel, x9[9 i + 1 + l] its
+// neighbour l (NaN: outside the volume).
+__global__ void __launch_bounds__(256) penalty_steps_kernel(int penalty, double lam, double del, uint64_t n,
+                                                            const double* __restrict__ alpha,
+                                                            const double* __restrict__ beta,
+                                                            const float* __restrict__ x9, double* __restrict__ out) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t i = warp; i < n; i += nwarps) {
+        const double xq = (double)x9[9 * i];
+        double diff = 0.0, wn = 0.0;
+        if (lane < 8) {
+            const float xn = x9[9 * i + 1 + lane];
+            if (!isnan(xn)) {
+                diff = (double)xn - xq;
+                wn = neighbour_weight(lane);
+            }
+        }
+        const double d = penalty_solve(penalty, lam, del, alpha[i], beta[i], diff, wn);
+        if (lane == 0) out[i] = d;
+    }
+}
+
 // One voxel update (work item `item` of a scan's visiting order) by one warp.
 template <class WT, int U = kU>
 __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* __restrict__ order,
                                              const int64_t* __restrict__ colptr, const uint32_t* __restrict__ vptr,
                                              const int32_t* __restrict__ idx, const WT* __restrict__ w,
                                              const int32_t* __restrict__ start, float* e, float* x, uint64_t item,
-                                             int lane) {
+                                             int lane, unsigned long long* scattered = nullptr) {
     const uint64_t ncol = (uint64_t)P.nx * P.ny;
     const uint32_t packed = __ldg(order + item);
     const uint64_t col = packed / (uint32_t)P.nz;
@@ -283,7 +404,7 @@ __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* _
         // physical position) all start their sweep at the data view where the
         // stack's last member's window begins, then wrap around, so they read
         // and update each sinogram sector at about the same time.
-        const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), P.last_slice[k % 2]);
+        const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
         const int vs = min(max(start[kl] - s, v0), v1);
         mid = cb + vp[vs];
     }
@@ -304,9 +425,21 @@ __device__ __forceinline__ void process_item(const GParams& P, const uint32_t* _
     if (lane == 0) x[q] = (float)(xq + upd);
     const float du = (float)upd;
     if (du != 0.f) {
+        // Reverse of the gather order: [b, mid) backwards, then [mid, en).
         const uint64_t drop = l2_drop();
-        scatter_range<WT, U>(idx, w, e, mid, en, off, lane, drop, du);
         scatter_range<WT, U>(idx, w, e, b, mid, off, lane, drop, du);
+        scatter_range<WT, U>(idx, w, e, mid, en, off, lane, drop, du);
+        if (scattered) *scattered += (unsigned long long)(en - b);
+    }
+}
+
+// Scatter counters of one launch, summed once per warp at exit:
+// [0] updates that scattered (du != 0), [1] matrix entries they scattered.
+__device__ __forceinline__ void flush_counts(unsigned long long* stats, unsigned long long upd,
+                                             unsigned long long ent, int lane) {
+    if (stats && lane == 0 && upd) {
+        atomicAdd(stats, upd);
+        atomicAdd(stats + 1, ent);
     }
 }
 
@@ -316,15 +449,109 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
                                                           const uint32_t* __restrict__ vptr,
                                                           const int32_t* __restrict__ idx,
                                                           const WT* __restrict__ w, const int32_t* __restrict__ start,
-                                                          float* e, float* x, unsigned long long* queue) {
+                                                          float* e, float* x, unsigned long long* queue,
+                                                          unsigned long long* stats) {
     const int lane = threadIdx.x & 31;
+    unsigned long long n_ent = 0, n_upd = 0;
     for (;;) {
         unsigned long long item = 0;
         if (lane == 0) item = atomicAdd(queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= P.n_items) break;
-        process_item<WT, U>(P, order, colptr, vptr, idx, w, start, e, x, item, lane);
+        const unsigned long long before = n_ent;
+        process_item<WT, U>(P, order, colptr, vptr, idx, w, start, e, x, item, lane, &n_ent);
+        n_upd += n_ent != before;
     }
+    flush_counts(stats, n_upd, n_ent, lane);
+}
+
+// Shared-memory staged variant: one warp per voxel update, NW warps per CTA,
+// each warp owning `cap` stage positions in shared memory. The gather reads
+// the column's matrix entries from HBM once, with a streaming (evict-first)
+// L2 policy so they do not displace the error sinogram, keeps each entry's
+// sinogram index (slice offset applied) and weight in the stage and gathers
+// e; after the penalty step the scatter reads the entries back from shared
+// memory, latest-gathered first (their e sectors are the likeliest to still
+// be in L2). Columns longer than `cap` re-read their tail from HBM.
+template <class WT, int U, int NW>
+__global__ void __launch_bounds__(32 * NW, 1) icd_staged_kernel(GParams P, const uint32_t* __restrict__ order,
+                                                                const int64_t* __restrict__ colptr,
+                                                                const uint32_t* __restrict__ vptr,
+                                                                const int32_t* __restrict__ idx,
+                                                                const WT* __restrict__ w,
+                                                                const int32_t* __restrict__ start, float* e, float* x,
+                                                                unsigned long long* queue, int cap,
+                                                                unsigned long long* stats) {
+    using SW = typename WBits<WT>::T;
+    extern __shared__ __align__(16) unsigned char stage_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t* sq = reinterpret_cast<int32_t*>(stage_smem) + (size_t)wid * cap;
+    SW* sw = reinterpret_cast<SW*>(reinterpret_cast<int32_t*>(stage_smem) + (size_t)NW * cap) + (size_t)wid * cap;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint64_t stream = l2_drop();
+    unsigned long long n_ent = 0, n_upd = 0;
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(queue, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= P.n_items) break;
+        const uint32_t packed = __ldg(order + item);
+        const uint64_t col = packed / (uint32_t)P.nz;
+        const int k = (int)(packed % (uint32_t)P.nz);
+        const int64_t q = (int64_t)col + (int64_t)ncol * k;
+        const int s = start[k];
+        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+        int64_t b = 0, en = 0, mid = 0;
+        if (v1 > v0) {
+            const int64_t cb = colptr[col];
+            const uint32_t* vp = vptr + col * P.nvsm1;
+            b = cb + vp[v0];
+            en = cb + vp[v1];
+            // Same common start view for the members of a slice stack as
+            // process_item.
+            const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
+            const int vs = min(max(start[kl] - s, v0), v1);
+            mid = cb + vp[vs];
+        }
+        const int off = s * P.nch * P.nr;
+        const int64_t n1 = en - mid, n = en - b;
+
+        float acc_b = 0.f, acc_a = 0.f;
+        stage_gather<WT, U>(idx, w, e, mid, en, 0, off, lane, stream, sq, sw, cap, acc_b, acc_a);
+        stage_gather<WT, U>(idx, w, e, b, mid, n1, off, lane, stream, sq, sw, cap, acc_b, acc_a);
+        const double beta = (double)warp_sum(acc_b);
+        const double alpha = (double)warp_sum(acc_a);
+
+        const double xq = (double)__ldcg(x + q);
+        double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+        if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+        if (lane == 0) x[q] = (float)(xq + upd);
+        const float du = (float)upd;
+        __syncwarp();  // stage writes of every lane visible to the scatter
+        if (du != 0.f) {
+            // Positions [cap, n) were not staged: re-read them (last first).
+            for (int64_t p = n - 1 - lane; p >= cap; p -= 32) {
+                const int64_t m = p < n1 ? mid + p : b + (p - n1);
+                atomicAdd(e + (ld_idx(idx + m, stream) + off), -du * WBits<WT>::value(WBits<WT>::load(w, m, stream)));
+            }
+            const int64_t ns = n < cap ? n : cap;
+            int64_t p = ns - 1 - lane;
+            for (; p >= 32 * 3; p -= 32 * 4) {
+                const int32_t q0 = sq[p], q1 = sq[p - 32], q2 = sq[p - 64], q3 = sq[p - 96];
+                const float w0 = WBits<WT>::value(sw[p]), w1 = WBits<WT>::value(sw[p - 32]);
+                const float w2 = WBits<WT>::value(sw[p - 64]), w3 = WBits<WT>::value(sw[p - 96]);
+                atomicAdd(e + q0, -du * w0);
+                atomicAdd(e + q1, -du * w1);
+                atomicAdd(e + q2, -du * w2);
+                atomicAdd(e + q3, -du * w3);
+            }
+            for (; p >= 0; p -= 32) atomicAdd(e + sq[p], -du * WBits<WT>::value(sw[p]));
+            n_ent += (unsigned long long)n;
+            ++n_upd;
+        }
+        __syncwarp();  // stage reads done before the next item overwrites it
+    }
+    flush_counts(stats, n_upd, n_ent, lane);
 }
 
 // CTA-per-voxel variant: WPV warps share one voxel update. Each thread keeps
@@ -339,8 +566,9 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
                                                         const uint32_t* __restrict__ vptr,
                                                         const int32_t* __restrict__ idx, const WT* __restrict__ w,
                                                         const int32_t* __restrict__ start, float* e, float* x,
-                                                        unsigned long long* queue) {
+                                                        unsigned long long* queue, unsigned long long* stats) {
     constexpr int NT = 32 * WPV;
+    unsigned long long n_ent = 0, n_upd = 0;
     constexpr int64_t CAP = (int64_t)NT * R;
     __shared__ unsigned long long s_item;
     __shared__ float s_red[2 * WPV + 1];
@@ -437,8 +665,12 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
                     if (m < en) atomicAdd(e + (__ldg(idx + m) + off), -du * ldw(w, m));
                 }
             }
+            n_ent += (unsigned long long)(en - b);
+            ++n_upd;
         }
+        __syncthreads();  // s_item / s_red reused by the next item
     }
+    flush_counts(stats, n_upd, n_ent, tid);
 }
 
 // Batched variant: one persistent launch drains the merged queue of several
@@ -566,8 +798,8 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     P.last_slice[(P.nz - 1) % 2] = P.nz - 1;
     P.last_slice[P.nz % 2] = P.nz >= 2 ? P.nz - 2 : P.nz - 1;
     P.n_items = rc->n_order;
-    P.lambda = (float)g.lambda;
-    P.delta = (float)g.delta;
+    P.lambda = g.lambda;
+    P.delta = g.delta;
     P.relax = (o.relax > 0.0 && o.relax < 2.0) ? o.relax : 1.0;
     P.cvx = g.center_voxel_x;
     P.cvy = g.center_voxel_y;
@@ -597,7 +829,11 @@ uint64_t max_items_in_flight(uint64_t n_items, int nz, int T) {
 // Voxel updates the options ask to keep in flight (warps_in_flight counts
 // warps; an update takes warps_per_voxel of them).
 uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o) {
-    const int W = o.warps_in_flight > 0 ? o.warps_in_flight : default_warps_in_flight(rc);
+    // The staged kernel keeps one CTA of 4 (or 8) updates per SM (its stage
+    // fills the SM's shared memory).
+    const int staged = rc->ctx->sm_count * (o.stage_column == 2 ? 8 : 4);
+    const int W = o.warps_in_flight > 0 ? o.warps_in_flight
+                                        : (o.stage_column ? staged : default_warps_in_flight(rc));
     const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     return std::max<uint64_t>(1, (uint64_t)(W / wpv));
 }
@@ -729,6 +965,24 @@ ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float
     return CTBB_OK;
 }
 
+template <class WT, int U, int NW>
+ctbb_status launch_staged(const GParams& P, const uint32_t* order, const ctbb_ssm* ssm, const WT* w, ctbb_recon* rc,
+                          uint64_t in_flight, unsigned long long* stats) {
+    ctbb_ctx* ctx = rc->ctx;
+    const int cap = stage_capacity(ctx, NW, (int)sizeof(WT));
+    const size_t smem = (size_t)NW * (size_t)cap * (4 + sizeof(WT));
+    CTBB_CUDA(cudaFuncSetAttribute(icd_staged_kernel<WT, U, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem));
+    // One CTA per SM is resident (the stage takes the SM's shared memory);
+    // a persistent grid larger than that would only add idle CTAs.
+    const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((in_flight + NW - 1) / NW, ctx->sm_count));
+    icd_staged_kernel<WT, U, NW><<<blocks, 32 * NW, smem, ctx->stream>>>(
+        P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx, w, rc->d_start, rc->d_e32, rc->d_x32, ctx->d_queue, cap,
+        stats);
+    return CTBB_OK;
+}
+
+
 // Build (or reuse) the full visiting order for tile edge P_lat.
 ctbb_status build_order(ctbb_recon* rc, int P_lat) {
     if (rc->d_order && rc->order_P == P_lat) return CTBB_OK;
@@ -775,8 +1029,18 @@ int default_warps_in_flight(const ctbb_recon* rc) {
     return std::max(4, std::min(rc->ctx->sm_count * 32, w));
 }
 
+// Stage positions per warp of the shared-memory staged kernel: what NW
+// warps' stages of (4-byte index + weight) entries fit in the opt-in shared
+// memory of one CTA, in whole warps' worth of entries.
+int stage_capacity(const ctbb_ctx* ctx, int nw, int wbytes) {
+    const size_t smem = ctx->smem_per_block_optin ? ctx->smem_per_block_optin : 48 * 1024;
+    const size_t per = smem / ((size_t)nw * (size_t)(4 + wbytes));
+    return (int)(per / 32 * 32);
+}
+
+
 ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o, float* ms,
-                               double* entries, uint64_t* items) {
+                               double* entries, uint64_t* items, double* scattered) {
     const int T = lattice_spacing(rc, o);
     CTBB_TRY(build_order(rc, T));
     if (o.priority && !rc->d_prio_order)
@@ -797,9 +1061,13 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     if (wpv != 1 && wpv != 4 && wpv != 8)
         return fail(CTBB_ERR_INVALID_ARG, "warps_per_voxel must be 1, 4 or 8 (got %d)", wpv);
+    const int stage = o.stage_column;
+    if (stage < 0 || stage > 2) return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0, 1 or 2 (got %d)", stage);
+    if (stage && wpv != 1) return fail(CTBB_ERR_INVALID_ARG, "stage_column needs one warp per voxel update");
     ctbb_ctx* ctx = rc->ctx;
     cudaStream_t st = ctx->stream;
-    CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, sizeof(unsigned long long), st));
+    unsigned long long* stats = ctx->d_queue + 2;
+    CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned long long), st));
     cudaEvent_t e0, e1;
     CTBB_CUDA(cudaEventCreate(&e0));
     CTBB_CUDA(cudaEventCreate(&e1));
@@ -811,39 +1079,56 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const int32_t* ix = ssm->d_idx;
     const int epl = o.entries_per_lane > 0 ? o.entries_per_lane : kU;
     if (epl != 8 && epl != 16) return fail(CTBB_ERR_INVALID_ARG, "entries_per_lane must be 8 or 16 (got %d)", epl);
-    if (wpv == 1) {
+    if (stage) {
+        // stage_column 1: 4 warps (updates) per CTA, 2: 8 (half the stage each).
+        if (stage == 1) {
+            if (h)
+                CTBB_TRY((epl == 16 ? launch_staged<__half, 16, 4> : launch_staged<__half, 8, 4>)(
+                    P, order, ssm, ssm->d_w16, rc, in_flight, stats));
+            else
+                CTBB_TRY((epl == 16 ? launch_staged<float, 16, 4> : launch_staged<float, 8, 4>)(
+                    P, order, ssm, ssm->d_w32, rc, in_flight, stats));
+        } else {
+            if (h)
+                CTBB_TRY((epl == 16 ? launch_staged<__half, 16, 8> : launch_staged<__half, 8, 8>)(
+                    P, order, ssm, ssm->d_w16, rc, in_flight, stats));
+            else
+                CTBB_TRY((epl == 16 ? launch_staged<float, 16, 8> : launch_staged<float, 8, 8>)(
+                    P, order, ssm, ssm->d_w32, rc, in_flight, stats));
+        }
+    } else if (wpv == 1) {
         const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
         if (epl == 16) {
             if (h)
                 icd_grouped_kernel<__half, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                       rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                       rc->d_e32, rc->d_x32, ctx->d_queue, stats);
             else
                 icd_grouped_kernel<float, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
         } else {
             if (h)
                 icd_grouped_kernel<__half, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
             else
                 icd_grouped_kernel<float, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
         }
     } else {
         const int blocks = (int)in_flight;
         if (wpv == 8) {
             if (h)
                 icd_cta_kernel<__half, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
             else
                 icd_cta_kernel<float, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
         } else {
             if (h)
                 icd_cta_kernel<__half, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
             else
                 icd_cta_kernel<float, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue);
+                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
         }
     }
     CTBB_CUDA(cudaGetLastError());
@@ -852,6 +1137,12 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     cudaEventElapsedTime(ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    if (scattered) {
+        unsigned long long h2[2] = {0, 0};
+        CTBB_CUDA(cudaMemcpyAsync(h2, stats, sizeof(h2), cudaMemcpyDeviceToHost, st));
+        CTBB_CUDA(cudaStreamSynchronize(st));
+        *scattered = (double)h2[1];
+    }
     return CTBB_OK;
 }
 
@@ -1136,5 +1427,47 @@ extern "C" ctbb_status ctbb_gpu_recon_set_priority(ctbb_recon* rc, const ctbb_ic
     rc->d_prio_order = order;
     rc->n_prio_order = n_order;
     rc->prio_P = T;
+    return CTBB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The grouped update's penalised 1-D solve on caller-given inputs.
+// ---------------------------------------------------------------------------
+extern "C" ctbb_status ctbb_gpu_penalty_steps(ctbb_ctx* ctx, int32_t penalty, double lambda, double delta,
+                                              uint64_t n, const double* alpha, const double* beta, const float* x9,
+                                              double* step) {
+    clear_error();
+    if (!ctx || (n && (!alpha || !beta || !x9 || !step))) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (penalty != CTBB_PENALTY_QUADRATIC && penalty != CTBB_PENALTY_EDGE_PRESERVING)
+        return fail(CTBB_ERR_INVALID_ARG, "unknown penalty %d", penalty);
+    if (n == 0) return CTBB_OK;
+    CTBB_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    double *d_a = nullptr, *d_b = nullptr, *d_out = nullptr;
+    float* d_x = nullptr;
+    auto cleanup = [&]() {
+        cudaFree(d_a);
+        cudaFree(d_b);
+        cudaFree(d_x);
+        cudaFree(d_out);
+    };
+    cudaError_t e = cudaMalloc(&d_a, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_b, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&d_x, 9 * n * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&d_out, n * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_a, alpha, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_b, beta, n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_x, x9, 9 * n * sizeof(float), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        const int grid = (int)std::min<uint64_t>((n + 7) / 8, (uint64_t)ctx->sm_count * 16);
+        penalty_steps_kernel<<<grid, 256, 0, st>>>(penalty, lambda, delta, n, d_a, d_b, d_x, d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(step, d_out, n * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cleanup();
+    if (e != cudaSuccess)
+        return fail(e == cudaErrorMemoryAllocation ? CTBB_ERR_OOM : CTBB_ERR_CUDA, "penalty steps: %s",
+                    cudaGetErrorString(e));
     return CTBB_OK;
 }

@@ -9,7 +9,7 @@
 // bit for bit; parity tests always feed the same raw buffer to both sides.
 //
 // Ray geometry (matches the stored-system-matrix model of
-// generate_system_matrix.cpp:205-241 and generate_system_matrix_ffs.cpp:104-151,
+// generate_system_matrix.cpp:85-116 and generate_system_matrix_ffs.cpp:112-153,
 // expressed in the fixed frame):
 //   view g:   theta_g = g * tube_angle_increment, source z = table_positions[g]
 //             S = (R cos theta_g, R sin theta_g, z_g)
@@ -19,7 +19,7 @@
 //   row r:     axial_r = (r - cr) * s_a
 //   detector point b = S - SDD cos(gamma) e_w - SDD sin(gamma) e_u - axial e_z
 //   FFS:       the ray starts at S + off, off = +da e_u (even g) / -da e_u (odd g),
-//              da = SDD R sin(fan_inc) / (4 (SDD - R))   (ffs.cpp:67, :250-259)
+//              da = SDD R sin(fan_inc) / (4 (SDD - R))   (generate_system_matrix_ffs.cpp:67, :250-259)
 #pragma once
 
 #include <math.h>

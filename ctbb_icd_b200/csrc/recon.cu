@@ -449,8 +449,10 @@ extern "C" ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ss
                 CTBB_CUDA(cudaGetLastError());
             }
             uint64_t items = 0;
-            CTBB_TRY(launch_icd_grouped(rc, ssm, *opts, &ms, &entries, &items));
+            double scattered = 0.0;
+            CTBB_TRY(launch_icd_grouped(rc, ssm, *opts, &ms, &entries, &items, &scattered));
             if (opts->priority) upd = (double)items;
+            s.entries_scattered += scattered;
         } else {
             return fail(CTBB_ERR_INVALID_ARG, "unknown ICD mode %d", opts->mode);
         }

@@ -131,11 +131,14 @@ extern "C" ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* 
 // the rotation kernel needs, lives in this fixed device array instead of a
 // cudaMalloc'd buffer.
 //
-// The array is a file-scope __device__ symbol, so every GPU that loads this
-// library holds it (2 * kNoAllocMaxSlices doubles, 128 KB) until the process
-// exits. Host code only knows the symbol's host-side shadow, so the device
-// address is looked up with cudaGetSymbolAddress once per device, with that
-// device current, the first time the entry point runs on it.
+// The array is a file-scope __device__ symbol (2 * kNoAllocMaxSlices doubles,
+// 128 KB): it is resident on each GPU from the library's first use there
+// (under CUDA's lazy module loading, the first call into it) until the
+// process exits. Host code only knows the symbol's host-side shadow, so the
+// device address is looked up with cudaGetSymbolAddress once per device,
+// with that device current, the first time the entry point runs on it, and
+// kept until exit (a caller's cudaDeviceReset would invalidate it; calls
+// after one are not supported).
 // ---------------------------------------------------------------------------
 namespace {
 

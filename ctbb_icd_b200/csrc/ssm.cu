@@ -50,7 +50,7 @@ struct SsmParams {
 // and the float weight when the ray contributes to column (ic, jc).
 __device__ __forceinline__ bool ray_weight(const SsmParams& P, const ViewTab& V, double A, double B,
                                            double ap, double nrm, int ic, int jc, float* wout) {
-    // gsm.cpp:236-239 / ffs.cpp:147-151 element by element.
+    // generate_system_matrix.cpp:111-114 / _ffs.cpp:147-151 element by element.
     double d0 = (A * V.ew0 - B * V.eu0) - ap * 0.0;
     double d1 = (A * V.ew1 - B * V.eu1) - ap * 0.0;
     double d2 = (A * 0.0 - B * 0.0) - ap * 1.0;
@@ -70,7 +70,7 @@ __device__ __forceinline__ bool ray_weight(const SsmParams& P, const ViewTab& V,
     d2 = d2 / n;
     const double aax = fabs(d0), aay = fabs(d1);
     if (aax > aay) {
-        // x-major: the ray is sampled on the line x = x_ic (gsm.cpp:256-279).
+        // x-major: the ray is sampled on the line x = x_ic (generate_system_matrix.cpp:127-155).
         const double x = (ic - P.cvx) * P.vx;
         const double y_hat = V.src1 + d1 / d0 * (x - V.src0);
         const double j_hat = y_hat / P.vy + P.cvy;
@@ -86,7 +86,7 @@ __device__ __forceinline__ bool ray_weight(const SsmParams& P, const ViewTab& V,
         *wout = (jj == jc) ? (float)(wz * (1 - (j_hat - jj))) : (float)(wz * (j_hat - jj));
         return true;
     } else {
-        // y-major: sampled on the line y = y_jc (gsm.cpp:285-308).
+        // y-major: sampled on the line y = y_jc (generate_system_matrix.cpp:156-184).
         const double y = (jc - P.cvy) * P.vy;
         const double x_hat = V.src0 + d0 / d1 * (y - V.src1);
         const double i_hat = x_hat / P.vx + P.cvx;
@@ -288,26 +288,26 @@ void host_tables(const ctbb_geom_c& g, std::vector<ViewTab>& vt, std::vector<dou
                  std::vector<double>& ap, std::vector<double>& nrm, bool ffs) {
     const size_t nvsm = g.num_views_for_system_matrix;
     const double SDD = g.source_detector_distance, R = g.focal_spot_radius;
-    const double da = SDD * R * sin(g.fan_angle_increment) / (4.0 * (SDD - R));  // ffs.cpp:67
+    const double da = SDD * R * sin(g.fan_angle_increment) / (4.0 * (SDD - R));  // generate_system_matrix_ffs.cpp:67
     vt.resize(nvsm);
     for (int i = 0; i < (int)nvsm; ++i) {
-        const double ta = (i - 0.5 * nvsm) * g.tube_angle_increment;  // gsm.cpp:210
+        const double ta = (i - 0.5 * nvsm) * g.tube_angle_increment;  // generate_system_matrix.cpp:85
         ViewTab& V = vt[i];
         V.ew0 = cos(ta);
         V.ew1 = sin(ta);
         V.eu0 = -sin(ta);
         V.eu1 = cos(ta);
         const double zs = g.table_direction * ((double)i - 0.5 * (double)nvsm) * g.tube_z_increment;
-        V.src0 = R * V.ew0 + zs * 0.0;  // gsm.cpp:225
+        V.src0 = R * V.ew0 + zs * 0.0;  // generate_system_matrix.cpp:100
         V.src1 = R * V.ew1 + zs * 0.0;
         V.src2 = R * 0.0 + zs * 1.0;
         V.off0 = V.off1 = V.off2 = 0.0;
         if (ffs) {
-            const double s = (i % 2 == 0) ? da : -da;  // ffs.cpp:253-259
+            const double s = (i % 2 == 0) ? da : -da;  // generate_system_matrix_ffs.cpp:253-259
             V.off0 = s * V.eu0;
             V.off1 = s * V.eu1;
             V.off2 = s * 0.0;
-            V.src0 = V.src0 + V.off0;  // ffs.cpp:134
+            V.src0 = V.src0 + V.off0;  // generate_system_matrix_ffs.cpp:134
             V.src1 = V.src1 + V.off1;
             V.src2 = V.src2 + V.off2;
         }
@@ -318,16 +318,16 @@ void host_tables(const ctbb_geom_c& g, std::vector<ViewTab>& vt, std::vector<dou
     for (int j = 0; j < (int)nch; ++j) {
         double tang;
         if (ffs)
-            tang = (j - g.center_channel_non_ffs) * g.fan_angle_increment;  // ffs.cpp:138
+            tang = (j - g.center_channel_non_ffs) * g.fan_angle_increment;  // generate_system_matrix_ffs.cpp:138
         else
-            tang = ((j - g.center_channel_non_ffs) * g.transaxial_detector_spacing) / SDD;  // gsm.cpp:228-229
+            tang = ((j - g.center_channel_non_ffs) * g.transaxial_detector_spacing) / SDD;  // generate_system_matrix.cpp:103-104
         A[j] = -SDD * cos(tang);
         B[j] = SDD * sin(tang);
     }
     ap.resize(nr);
     nrm.resize(nr);
     for (int k = 0; k < (int)nr; ++k) {
-        ap[k] = (k - g.center_row) * g.axial_detector_spacing;  // gsm.cpp:234
+        ap[k] = (k - g.center_row) * g.axial_detector_spacing;  // generate_system_matrix.cpp:109
         nrm[k] = sqrt(ap[k] * ap[k] + SDD * SDD);
     }
 }

@@ -48,28 +48,36 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
 
     // Candidates (warps per voxel, warps in flight, entries per lane, tile
-    // edge): one warp per voxel at 1/4 .. 2 times the coupling-bound default,
-    // 8 or 16 entries per lane in flight, the default tile edge for that
-    // concurrency (and half of it at the default); 4 warps per voxel with
-    // four updates per SM. Launches cap the updates in flight at the visiting
-    // order's bound, so candidates that collapse onto the same effective
-    // shape run once.
+    // edge, column stage): the shared-memory staged kernel with 4 or 8
+    // updates per SM; one warp per voxel streaming the column twice at
+    // 1/4 .. 2 times the coupling-bound default; 8 or 16 entries per lane in
+    // flight, the default tile edge for that concurrency (and half of it);
+    // 4 warps per voxel with four updates per SM. Launches cap the updates in
+    // flight at the visiting order's bound, so candidates that collapse onto
+    // the same effective shape run once.
     const int w0 = default_warps_in_flight(rc);
     const int sms = rc->ctx->sm_count;
     const int wmax = sms * 48;
     struct Cand {
-        int wpv, w, epl, half;
+        int wpv, w, epl, half, stage;
     };
     std::vector<Cand> cands;
+    // Shared-memory staged kernels first: one CTA per SM with 4 (or 8)
+    // updates, the matrix read once per update.
+    for (int epl : {16, 8}) {
+        cands.push_back({1, 4 * sms, epl, 0, 1});
+        cands.push_back({1, 8 * sms, epl, 0, 2});
+    }
+    cands.push_back({1, 4 * sms, 16, 1, 1});
     for (int epl : {8, 16})
         for (int m4 : {1, 2, 4, 8}) {
             const int w = std::max(32, std::min(wmax, w0 * m4 / 4));
-            cands.push_back({1, w, epl, 0});
-            if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1});
+            cands.push_back({1, w, epl, 0, 0});
+            if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1, 0});
         }
-    cands.push_back({4, 4 * sms * 4, 8, 0});
+    cands.push_back({4, 4 * sms * 4, 8, 0, 0});
     struct Trial {
-        int wpv, w, epl, t;
+        int wpv, w, epl, t, stage;
         double ms, cost, score;
     };
     std::vector<Trial> trials;
@@ -81,6 +89,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             c.warps_in_flight = cd.w;
             c.warps_per_voxel = cd.wpv;
             c.entries_per_lane = cd.epl;
+            c.stage_column = cd.stage;
             c.lattice = 0;
             const int t_auto = lattice_spacing(rc, c);
             c.lattice = cd.half ? std::max(4, t_auto / 2) : t_auto;
@@ -92,7 +101,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             bool seen = false;
             for (const Trial& tr : trials)
                 seen |= tr.wpv == c.warps_per_voxel && tr.w == c.warps_in_flight && tr.t == c.lattice &&
-                        tr.epl == c.entries_per_lane;
+                        tr.epl == c.entries_per_lane && tr.stage == c.stage_column;
             if (seen) continue;
             if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
                 status = fail(CTBB_ERR_CUDA, "autotune restore");
@@ -110,7 +119,8 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             if (status == CTBB_OK) status = cost_f64(rc, ssm, false, &cost);
             if (status != CTBB_OK) break;
             const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
-            trials.push_back({c.warps_per_voxel, c.warps_in_flight, c.entries_per_lane, c.lattice, ms_tot, cost, score});
+            trials.push_back(
+                {c.warps_per_voxel, c.warps_in_flight, c.entries_per_lane, c.lattice, c.stage_column, ms_tot, cost, score});
             if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
         }
     }
@@ -125,6 +135,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     best->warps_in_flight = trials[ibest].w;
     best->warps_per_voxel = trials[ibest].wpv;
     best->entries_per_lane = trials[ibest].epl;
+    best->stage_column = trials[ibest].stage;
     best->lattice = trials[ibest].t;
     if (report) {
         memset(report, 0, sizeof(*report));
@@ -135,6 +146,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             report->trials[i].warps_in_flight = trials[i].w;
             report->trials[i].warps_per_voxel = trials[i].wpv;
             report->trials[i].entries_per_lane = trials[i].epl;
+            report->trials[i].stage_column = trials[i].stage;
             report->trials[i].lattice = trials[i].t;
             report->trials[i].device_ms = trials[i].ms;
             report->trials[i].cost = trials[i].cost;

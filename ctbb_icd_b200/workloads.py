@@ -91,6 +91,17 @@ WORKLOADS = {
              **_recon(512, 30.0, 0.06, 64, -3.0, "edge-preserving", 0.1, 9.6e-4, 10)},
         phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
     ),
+    # cfg2 on its central 15 cm: scanner, views, flying focal spot, voxel
+    # size, slab (64 slices) and penalty of the full workload at 256 x 256
+    # (a quarter of its voxels; about 5 GB on the device with FP16 weights):
+    # the kernel-profiling case whose per-update footprint and slab height
+    # match the benchmark's.
+    "cfg2_quarter": dict(
+        prm={**_BASE,
+             **_scanner(736, 366.25, FAN_INC, 64, 0.06, 1152, True, 1.0, 4),
+             **_recon(256, 15.0, 0.06, 64, -3.0, "edge-preserving", 0.1, 9.6e-4, 10)},
+        phantom=dict(n_ellipsoids=40, seed=0, i0_lo=5e4, i0_hi=2e5),
+    ),
     # cfg2's scanner, views, flying focal spot and penalty over the full 30 cm
     # FOV at 128 x 128 (2.3 mm voxels) x 16 slices of 0.6 mm, two turns.
     "cfg2_lite": dict(

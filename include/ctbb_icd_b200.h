@@ -282,8 +282,27 @@ typedef struct ctbb_icd_opts {
                                  between gather and scatter                       */
     int32_t entries_per_lane; /* grouped, one warp per voxel: matrix entries each lane
                                  keeps in flight per round trip, 8 (0) or 16      */
-    int32_t reserved3;
+    int32_t stage_column;     /* grouped, one warp per voxel: 0 reads the column's
+                                 matrix entries from HBM for the gather and again
+                                 for the scatter; 1 keeps them in a shared-memory
+                                 stage between the two (4 updates per CTA), 2 the
+                                 same with 8 updates per CTA and half the stage   */
 } ctbb_icd_opts;
+
+/*
+ * The grouped mode's penalised one-voxel update on caller-given inputs, for
+ * verification: for each of n voxels, the surrogate numerator beta[i] and
+ * denominator alpha[i] of icd_iteration.cpp:198-209, the voxel value
+ * x9[9 i] and its 8 in-plane neighbours x9[9 i + 1 + l] in the order
+ * {-nx-1, -nx, -nx+1, -1, +1, nx-1, nx, nx+1} of penalties.cpp:41-52 (NaN
+ * marks a neighbour outside the volume), returns in step[i] the update
+ * before the positivity clamp: the closed form of quadratic()
+ * (penalties.cpp:61-85), or the root of edge_preserving()'s surrogate
+ * equation (penalties.cpp:88-154), found by safeguarded Newton inside the
+ * reference's bisection bracket. Host buffers; the call synchronises.
+ */
+ctbb_status ctbb_gpu_penalty_steps(ctbb_ctx* ctx, int32_t penalty, double lambda, double delta, uint64_t n,
+                                   const double* alpha, const double* beta, const float* x9, double* step);
 
 typedef struct ctbb_iter_stats {
     int32_t iterations;       /* iterations run by the call                       */
@@ -293,6 +312,8 @@ typedef struct ctbb_iter_stats {
     double device_ms;         /* device time of the ICD kernels in the call       */
     double voxel_updates;     /* voxel updates performed                          */
     double entries;           /* SSM entries visited (sum of in-range nnz)        */
+    double entries_scattered; /* grouped: entries of the updates that changed their
+                                 voxel and so scattered into e (du != 0)          */
 } ctbb_iter_stats;
 
 /*
@@ -378,13 +399,16 @@ ctbb_status ctbb_gpu_rotate_device(ctbb_ctx* ctx, const ctbb_geom_c* geom,
  * bound loops that cannot afford the allocator's implicit synchronisation,
  * or hosts that cap the process's device footprint. The only scratch the
  * rotation needs, the per-slice cos/sin table, is kept in a fixed device
- * array of 2 x 8192 doubles (128 KB) that every GPU loading this library
- * holds until the process exits; volumes of more than 8192 slices are
+ * array of 2 x 8192 doubles (128 KB), resident on each GPU from the
+ * library's first use there until the process exits; volumes of more than 8192 slices are
  * rejected with CTBB_ERR_INVALID_ARG. Input and output stay caller-owned
  * device buffers and give the same result as ctbb_gpu_rotate_device.
  *
  * The first call on each device looks up the array's device address, so
- * make that first call before any stream capture starts. All calls share the
+ * make that first call before any stream capture starts. Every call
+ * synchronises ctx's stream before it returns. The looked-up address is kept
+ * for the life of the process: a cudaDeviceReset by the caller invalidates
+ * it, and calls after such a reset are not supported. All calls share the
  * one array: calls whose work overlaps on the GPU (other host threads or
  * streams of the same device) race on it. Each call rewrites the entries it
  * uses, so nothing left by an earlier call leaks into a later one.
@@ -416,6 +440,8 @@ typedef struct ctbb_tune_trial {
     int32_t warps_per_voxel;
     int32_t lattice;
     int32_t entries_per_lane;
+    int32_t stage_column;
+    int32_t reserved;
     double device_ms;   /* ICD kernel time of the probe iterations */
     double cost;        /* FP64 cost after them                    */
     double score;       /* (start_cost - cost) / device_ms         */

@@ -18,10 +18,15 @@ extern "C" {
 
 typedef struct port_ssm port_ssm;
 
-// Stored system matrix, ray-driven like generate_system_matrix.cpp:205-311 and
-// generate_system_matrix_ffs.cpp:104-230 (FFS chosen by geom->Phiffs).
+// Stored system matrix, ray-driven like generate_system_matrix.cpp:80-186 and
+// generate_system_matrix_ffs.cpp:104-222 (FFS chosen by geom->Phiffs).
 port_ssm* port_ssm_build(const ctbb_geom_c* geom);
 uint64_t port_ssm_nnz(const port_ssm* s);
+// The entries of selected columns on selected (ascending) views only, same
+// arithmetic; counts[c * n_views + v] per (column, view), entries written in
+// that order up to `capacity`. Returns the total entry count.
+uint64_t port_ssm_subset(const ctbb_geom_c* geom, int n_cols, const int64_t* cols, int n_views,
+                         const int32_t* views, uint32_t* counts, int32_t* idx, float* w, uint64_t capacity);
 void port_ssm_copy(const port_ssm* s, int64_t* colptr, int32_t* idx, float* w);
 void port_ssm_free(port_ssm* s);
 
@@ -50,6 +55,12 @@ void port_forward(const ctbb_geom_c* geom, const uint64_t* slice_indices, const 
 double port_cost(const ctbb_geom_c* geom, const uint64_t* slice_indices, const float* raw,
                  const int64_t* colptr, const int32_t* idx, const float* w, const double* x,
                  double* data_term, double* penalty_term);
+
+// The reference's penalised one-voxel update (penalties.cpp:61-154) on given
+// inputs: x9[9 i] the voxel, x9[9 i + 1 + l] its neighbour l in the order
+// {-nx-1, -nx, -nx+1, -1, +1, nx-1, nx, nx+1} (NaN: outside the volume).
+void port_penalty_steps(int penalty, double lambda, double delta, uint64_t n, const double* alpha,
+                        const double* beta, const float* x9, double* step);
 
 // Synthetic raw data on the CPU (phantom.h), raw[Readings][n_ch][n_rows].
 void port_synth(const ctbb_geom_c* geom, const ctbb_phantom_spec* spec, float* raw);

@@ -6,47 +6,20 @@ from __future__ import annotations
 import ctypes as C
 import os
 import subprocess
+import sys
 
 import numpy as np
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-PORT_LIB = os.path.join(ROOT, "oracle", "_ref", "liboracle_port.so")
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "icd_ref_O2")
 REF_BIN_SHIPPED = os.path.join(ROOT, "oracle", "_ref", "icd_ref")
+REF_BIN_CORES = os.path.join(ROOT, "oracle", "_ref", "icd_ref_cores")
 REF_SETUP_DUMP = os.path.join(ROOT, "oracle", "_ref", "ref_setup_dump")
 
-_port = None
-
-
-def port():
-    global _port
-    if _port is None:
-        from ctbb_icd_b200._lib import GeomC, PhantomSpec
-
-        if not os.path.exists(PORT_LIB):
-            subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "port"], check=True)
-        L = C.CDLL(PORT_LIB)
-        PG = C.POINTER(GeomC)
-        PD, PF, PU, PI, PI64 = (C.POINTER(C.c_double), C.POINTER(C.c_float), C.POINTER(C.c_uint64),
-                                C.POINTER(C.c_int32), C.POINTER(C.c_int64))
-        L.port_ssm_build.restype = C.c_void_p
-        L.port_ssm_build.argtypes = [PG]
-        L.port_ssm_nnz.restype = C.c_uint64
-        L.port_ssm_nnz.argtypes = [C.c_void_p]
-        L.port_ssm_copy.argtypes = [C.c_void_p, PI64, PI, PF]
-        L.port_ssm_free.argtypes = [C.c_void_p]
-        L.port_icd.argtypes = [PG, PU, PF, PI64, PI, PF, PD, PD, C.c_int, PD]
-        L.port_rotate.argtypes = [PG, PD, PU, PF, C.c_int]
-        L.port_forward.argtypes = [PG, PU, PI64, PI, PF, PD, PD]
-        L.port_cost.restype = C.c_double
-        L.port_cost.argtypes = [PG, PU, PF, PI64, PI, PF, PD, PD, PD]
-        L.port_synth.argtypes = [PG, C.POINTER(PhantomSpec), PF]
-        _port = L
-    return _port
-
-
-def _p(a, t):
-    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+from oracle.port_binding import PORT_LIB, port  # noqa: E402
+from oracle.port_binding import ptr as _p  # noqa: E402
 
 
 class Csr:
@@ -77,6 +50,38 @@ def port_ssm(rp) -> Csr:
     finally:
         L.port_ssm_free(h)
     return Csr(colptr, idx, w)
+
+
+def port_ssm_subset(rp, cols, views):
+    """Entries of the given columns restricted to the given SSM views (the
+    oracle's ray-driven builder evaluated only where it reaches them).
+    Returns {column: (idx int32, w float32)} in the reference's entry order."""
+    L = port()
+    cols = np.ascontiguousarray(cols, np.int64)
+    views = np.ascontiguousarray(np.sort(np.asarray(views)), np.int32)
+    counts = np.zeros(len(cols) * len(views), np.uint32)
+    cap = 1 << 16
+    while True:
+        idx = np.empty(cap, np.int32)
+        w = np.empty(cap, np.float32)
+        n = int(L.port_ssm_subset(C.byref(rp.geom), len(cols), _p(cols, C.c_int64), len(views),
+                                  _p(views, C.c_int32), counts.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                  _p(idx, C.c_int32), _p(w, C.c_float), cap))
+        if n <= cap:
+            break
+        cap = n
+    out, pos = {}, 0
+    per_col = counts.reshape(len(cols), len(views)).sum(axis=1)
+    for c, m in zip(cols, per_col):
+        out[int(c)] = (idx[pos:pos + m].copy(), w[pos:pos + m].copy())
+        pos += int(m)
+    return out
+
+
+def restrict_views(idx, w, views, n_per_view):
+    """Entries of a column whose matrix view (q // (n_channels * Nrows)) is in `views`."""
+    keep = np.isin(idx // n_per_view, np.asarray(views))
+    return idx[keep], w[keep]
 
 
 def port_icd(rp, slice_indices, raw, ssm: Csr, n_iter, x0=None, est0=None):
@@ -180,3 +185,67 @@ def run_reference(prm_path, workdir, binary=REF_BIN, threads=None, timeout=3600)
     if r.returncode != 0:
         raise RuntimeError(f"reference exited {r.returncode}: {r.stdout[-2000:]}")
     return r.stdout
+
+
+def column_hashes(path, ncol):
+    """Per column of a matrix.bin: (entry count, 64-bit BLAKE2b of the
+    column's count and records)."""
+    import hashlib
+
+    buf = np.fromfile(path, np.uint8)
+    counts = np.zeros(ncol, np.int64)
+    hashes = np.zeros(ncol, np.uint64)
+    pos = 0
+    for c in range(ncol):
+        n = int(buf[pos:pos + 8].view(np.uint64)[0])
+        end = pos + 8 + 8 * n
+        counts[c] = n
+        hashes[c] = np.frombuffer(hashlib.blake2b(buf[pos:end].tobytes(), digest_size=8).digest(), np.uint64)[0]
+        pos = end
+    if pos != buf.size:
+        raise ValueError(f"{path}: {buf.size - pos} trailing bytes")
+    return counts, hashes
+
+
+def raw_hash(raw):
+    import hashlib
+
+    return hashlib.blake2b(np.ascontiguousarray(raw, np.float32).tobytes(), digest_size=16).hexdigest()
+
+
+def bench_size_fixture(name, directory):
+    """Materialise a benchmark-size golden fixture (make_golden.py cfg1 /
+    cfg2_sub) in `directory`: the parameter file, and the raw frames
+    regenerated with the oracle projector on the reference's own geometry
+    (checked against the fixture's hash). Returns (npz, prm_path)."""
+    import ast
+
+    from oracle import reference_run as R
+
+    z = np.load(os.path.join(ROOT, "tests", "golden", f"{name}.npz"))
+    text = str(z["prm"]).replace("@DIR@", directory)
+    prm_path = os.path.join(directory, f"{name}.prm")
+    with open(prm_path, "w") as f:
+        f.write(text)
+    kv = dict(line.split(": ", 1) for line in text.splitlines() if ": " in line and not line.startswith("#"))
+    R.write_zero_raw(kv["sinogram_path"], int(kv["Readings"]), int(kv["n_channels"]), int(kv["Nrows"]))
+    fields, _, _ = R.setup_dump(prm_path)
+    raw = R.synth_raw(R.geometry(fields), ast.literal_eval(str(z["phantom"])))
+    if raw_hash(raw) != str(z["raw_hash"]):
+        raise AssertionError(f"{name}: regenerated raw frames differ from the fixture's")
+    R.write_raw(kv["sinogram_path"], raw)
+    os.makedirs(os.path.join(directory, "reconstructions"), exist_ok=True)
+    return z, prm_path
+
+
+def port_penalty_steps(penalty, lam, delta, alpha, beta, x9):
+    """The reference's one-voxel penalised update (penalties.cpp:61-154) on
+    given inputs; x9 [n, 9] = voxel and 8 neighbours (NaN: outside)."""
+    a = np.ascontiguousarray(alpha, np.float64)
+    b = np.ascontiguousarray(beta, np.float64)
+    x = np.ascontiguousarray(x9, np.float32).reshape(-1, 9)
+    out = np.empty(a.size, np.float64)
+    port().port_penalty_steps(int(penalty), float(lam), float(delta), a.size, _p(a, C.c_double), _p(b, C.c_double),
+                              _p(x, C.c_float), _p(out, C.c_double))
+    return out
+

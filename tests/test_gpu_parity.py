@@ -196,15 +196,17 @@ def converged_cfg1_small(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights,wpv", [(C.SSM_FP32, 1), (C.SSM_FP16, 1), (C.SSM_FP32, 8), (C.SSM_FP16, 4)])
-def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv):
+@pytest.mark.parametrize("weights,wpv,stage", [(C.SSM_FP32, 1, 0), (C.SSM_FP16, 1, 0), (C.SSM_FP32, 8, 0),
+                                               (C.SSM_FP16, 4, 0), (C.SSM_FP16, 1, 1), (C.SSM_FP32, 1, 2)])
+def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage):
     rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
     rc = C.Recon(rp, data.slice_indices, ctx)
     rc.set_raw(data.raw)
     rc.set_volume(ssm, None)
     costs = []
     for _ in range(6):
-        rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5, warps_per_voxel=wpv))
+        rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5, warps_per_voxel=wpv,
+                                      stage_column=stage))
         rc.refresh_residual(ssm)
         costs.append(rc.cost())
     x = rc.volume_f64()
@@ -247,3 +249,51 @@ def test_batch_of_uneven_scans_converges(ctx, converged_cfg1_small, tmp_path):
         r.refresh_residual(s)
         assert r.cost() < c15 < c0, (c0, c15, r.cost())
     batch.free()
+
+
+@pytest.fixture(scope="module")
+def converged_small_ffs(ctx, tmp_path_factory):
+    """small_ffs (in-plane flying focal spot, edge-preserving penalty,
+    32 x 32 x 6): the sequential-order ICD image run until it moves less than
+    0.01 HU over 50 iterations, and its FP64 cost (the penalty is convex, so
+    this optimum is the one any visiting order must reach)."""
+    prm, rp = W.materialise("small_ffs", str(tmp_path_factory.mktemp("small_ffs_conv")))
+    data = C.load_raw(rp)
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_BOTH)
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    prev, moved = None, None
+    for _ in range(60):
+        rc.iterate(ssm, 50, C.icd_opts(mode=C.ICD_SEQUENTIAL))
+        x = rc.volume_f64()
+        if prev is not None:
+            moved = np.abs(x - prev).max() / HU
+            if moved < 0.01:
+                break
+        prev = x
+    assert moved is not None and moved < 0.01, moved
+    x_ref, cost_ref = rc.volume_f64(), rc.cost()
+    rc.free()
+    return rp, data, ssm, x_ref, cost_ref
+
+
+@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1)])
+def test_grouped_edge_preserving_reaches_converged_cost(ctx, converged_small_ffs, weights, stage):
+    rp, data, ssm, x_ref, cost_ref = converged_small_ffs
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    costs = []
+    rmse_hu = None
+    for _ in range(60):
+        rc.iterate(ssm, 25, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5, stage_column=stage))
+        rc.refresh_residual(ssm)
+        costs.append(rc.cost())
+        rmse_hu = np.sqrt(np.mean((rc.volume_f64() - x_ref) ** 2)) / HU
+        if rmse_hu <= 0.1 and abs(costs[-1] - cost_ref) <= 1e-7 * abs(cost_ref):
+            break
+    assert all(b <= a * (1 + 1e-9) for a, b in zip(costs, costs[1:])), costs
+    assert rmse_hu <= 0.5, rmse_hu
+    assert abs(costs[-1] - cost_ref) <= 1e-6 * abs(cost_ref), (costs[-1], cost_ref)
+    rc.free()

@@ -80,3 +80,23 @@ def test_port_forward_is_linear(golden):
     f2 = O.port_forward(golden.rp, golden.data.slice_indices, m, x2)
     f12 = O.port_forward(golden.rp, golden.data.slice_indices, m, 2 * x1 + 3 * x2)
     assert np.allclose(f12, 2 * f1 + 3 * f2, rtol=1e-12, atol=1e-12)
+
+
+def test_port_ssm_subset_equals_full_build_restricted(tmp_path):
+    """The column/view-restricted builder (used to check the full-size matrix
+    on sampled columns) gives exactly the full builder's entries."""
+    for name in ("tiny", "tiny_ffs", "small_ffs"):
+        _, rp = W.materialise(name, str(tmp_path / name), raw=False)
+        full = O.port_ssm(rp)
+        ncol = int(rp.geom.nx * rp.geom.ny)
+        nvsm = int(rp.geom.num_views_for_system_matrix)
+        per_view = int(rp.geom.n_channels * rp.geom.Nrows_projection)
+        rng = np.random.default_rng(11)
+        cols = np.unique(np.concatenate([[0, ncol - 1], rng.integers(0, ncol, 24)]))
+        views = np.unique(np.concatenate([[0, nvsm - 1], rng.integers(0, nvsm, max(4, nvsm // 5))]))
+        sub = O.port_ssm_subset(rp, cols, views)
+        for c in cols:
+            ri, rw = O.restrict_views(*full.column(int(c)), views, per_view)
+            si, sw = sub[int(c)]
+            assert np.array_equal(si, ri), (name, c)
+            assert np.array_equal(sw.view(np.int32), rw.view(np.int32)), (name, c)
