@@ -304,8 +304,8 @@ def run_stage(args):
     workdir = tempfile.mkdtemp(prefix="ctbb_stage_")
     peak, peak_kind = measured_peak()
     clocks = ClockSampler(0, enabled=args.clocks)
-    if args.stage == "cnn":
-        line = _stage_cnn(args, C, ctx, torch, clocks)
+    if args.stage in ("cnn", "batch"):
+        line = (_stage_cnn if args.stage == "cnn" else _stage_batch)(args, C, ctx, torch, clocks)
         line.update({"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
                      "data": "synthetic", "clocks": clocks.summary()})
         ctx.close()
@@ -373,6 +373,111 @@ def run_stage(args):
     ctx.close()
     subprocess.run(["rm", "-rf", workdir])
     return line
+
+
+def _stage_batch(args, C, ctx, torch, clocks):
+    """--stage batch: the benchmark's config 4, 32 independent uneven scans
+    (replicas.batch_specs: 128..512 squared, 8..64 rows, pitch 0.5..1.5, with
+    or without the in-plane flying focal spot, 8..64 slices, random
+    ellipsoids, quadratic penalty, FP32 weights), 20 iterations each, on one
+    GPU through the batched persistent kernel (one launch per iteration for
+    all scans of a batch, replayed from a CUDA graph). Scans are packed into
+    batches that fit in device memory (a scan that does not fit starts the
+    next batch). For each batch the first three iterations try 0.5, 1 and 2
+    times the default concurrency and the remaining 17 use the fastest.
+    Metric: voxel updates of all scans over the device time of the ICD
+    launches; the wall-clock rate including each scan's set-up (projector,
+    matrix build, visiting order) is reported beside it."""
+    from ctbb_icd_b200 import replicas as RP
+    from ctbb_icd_b200 import workloads as W
+
+    specs = RP.batch_specs(32, seed=0)
+    order = sorted(range(len(specs)), key=lambda i: -RP.scan_cost(specs[i]))
+    workdir = tempfile.mkdtemp(prefix="ctbb_batch_")
+    n_iter = 20
+    totals = {"updates": 0.0, "device_ms": 0.0, "entries": 0.0}
+    batches = []
+    t_wall = time.perf_counter()
+    clocks.start()
+    pending = list(order)
+    while pending:
+        scans = []
+        while pending:
+            i = pending[0]
+            sp = specs[i]
+            d = os.path.join(workdir, sp["name"])
+            os.makedirs(d, exist_ok=True)
+            prm = dict(sp["prm"], sinogram_path=os.path.join(d, "raw.bin"), output_dir=d, output_file="o.img")
+            open(prm["sinogram_path"], "wb").close()
+            rp = C.configure_recon_params(W.write_prm(os.path.join(d, "s.prm"), prm))
+            rc = ssm = None
+            try:
+                tables = C.slice_tables(rp)
+                rc = C.Recon(rp, tables.slice_indices, ctx)
+                ph = W.phantom_spec(dict(sp["phantom"], z_lo=min(prm["z_start"], prm["z_end"]),
+                                         z_hi=max(prm["z_start"], prm["z_end"])))
+                C.check(C.lib().ctbb_gpu_synth_raw(ctx.handle, ctypes.byref(rp.geom), ctypes.byref(ph),
+                                                   ctypes.c_void_p(rc.raw_device_ptr())))
+                ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
+                rc.set_volume(ssm, None)
+            except C.CtbbError as e:
+                for obj in (ssm, rc):
+                    if obj is not None:
+                        obj.free()
+                if e.status != 7 or not scans:  # CTBB_ERR_OOM with scans pending: run them first
+                    raise
+                break
+            scans.append((i, rp, rc, ssm))
+            pending.pop(0)
+        b = C.Batch([x[2] for x in scans], [x[3] for x in scans], ctx)
+        n_vox = sum(int(np.prod(x[1].shape)) for x in scans)
+        base = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
+        default_w = _batch_default_warps(ctx, [x[1] for x in scans])
+        st0 = b.iterate(1, base)
+        trials = [(default_w, st0.device_ms, st0.entries)]
+        for mult in (0.5, 2.0):
+            w = max(4, int(default_w * mult))
+            st = b.iterate(1, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=w))
+            trials.append((w, st.device_ms, st.entries))
+        best_w = min(trials, key=lambda t: t[1])[0]
+        st = b.iterate(n_iter - 3, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=best_w))
+        dev_ms = sum(t[1] for t in trials) + st.device_ms
+        totals["updates"] += n_vox * n_iter
+        totals["device_ms"] += dev_ms
+        totals["entries"] += sum(t[2] for t in trials) + st.entries
+        costs = []
+        for _, _, rc, ssm in scans:
+            rc.refresh_residual(ssm)
+            costs.append(rc.cost())
+        batches.append({"scans": [specs[x[0]]["name"] for x in scans], "voxels": n_vox,
+                        "warps_in_flight": best_w, "trials_ms": [[t[0], round(t[1], 2)] for t in trials],
+                        "device_ms": round(dev_ms, 1)})
+        b.free()
+        for _, _, rc, ssm in scans:
+            rc.free()
+            ssm.free()
+        torch.cuda.synchronize()
+    clocks.stop()
+    wall = time.perf_counter() - t_wall
+    subprocess.run(["rm", "-rf", workdir])
+    value = totals["updates"] / (totals["device_ms"] / 1e3)
+    return {"metric": "voxel-updates/s", "value": value, "unit": "voxel-updates/s",
+            "ms_per_step": totals["device_ms"] / n_iter, "dtype": "f32",
+            "config": {"workload": "32 uneven helical scans (config 4), 20 iterations each, quadratic penalty, "
+                                   "FP32 weights, batched persistent kernel replayed from a CUDA graph",
+                       "stage": "batch", "scans": len(specs), "batches": batches,
+                       "voxel_updates": totals["updates"], "entries": totals["entries"],
+                       "wall_s_including_setup": round(wall, 1),
+                       "wall_rate_including_setup": totals["updates"] / wall}}
+
+
+def _batch_default_warps(ctx, rps):
+    """The batch kernel's default concurrency (icd_grouped.cu
+    ctbb_gpu_batch_iterate): 0.4 x voxels / (3.2 x largest nx), within
+    [4, 32 warps per SM]."""
+    n = sum(float(np.prod(r.shape)) for r in rps)
+    nx = max(int(r.geom.nx) for r in rps)
+    return max(4, min(148 * 32, int(0.4 * n / (3.2 * nx))))
 
 
 def _stage_cnn(args, C, ctx, torch, clocks):
@@ -648,9 +753,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
     ap.add_argument("--no-clocks", dest="clocks", action="store_false", help="skip nvidia-smi clock sampling")
     ap.add_argument("--own-stream", action="store_true", help="run on the library's own stream")
-    ap.add_argument("--stage", choices=["icd", "ssm", "rotate", "cnn"], default="icd",
+    ap.add_argument("--stage", choices=["icd", "ssm", "rotate", "cnn", "batch"], default="icd",
                     help="icd (default): the grouped-ICD benchmark; ssm / rotate: time the matrix builder or the "
-                         "slice rotation of the same workload on their own; cnn: the warm-start network")
+                         "slice rotation of the same workload on their own; cnn: the warm-start network; "
+                         "batch: 32 uneven scans (config 4)")
     ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
     ap.add_argument("--stage-column", type=int, default=-1,
                     help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory")

@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._lib import (  # noqa: F401
-    ICD_GROUPED, ICD_SEQUENTIAL, PENALTY_EDGE_PRESERVING, PENALTY_QUADRATIC,
+    ESTIMATE_FORWARD, ESTIMATE_ZERO, ICD_GROUPED, ICD_SEQUENTIAL, PENALTY_EDGE_PRESERVING, PENALTY_QUADRATIC,
     ROTATE_FIXED2ROTATING, ROTATE_ROTATING2FIXED, SSM_BOTH, SSM_FP16, SSM_FP32, CtbbError,
     GeomC, IcdOpts, IterStats, PhantomSpec, PrmStrings, SsmInfo, check, lib, ptr,
 )
@@ -307,9 +307,12 @@ class Recon:
     def raw_device_ptr(self) -> int:
         return lib().ctbb_gpu_recon_raw_device(self.handle) or 0
 
-    def set_volume(self, ssm: Ssm, vol: np.ndarray | None = None):
+    def set_volume(self, ssm: Ssm, vol: np.ndarray | None = None, estimate: int = ESTIMATE_FORWARD):
+        """Set the iterate (zeros if vol is None) and the sinogram estimate:
+        ESTIMATE_FORWARD y_hat = A x, ESTIMATE_ZERO y_hat = 0 (the reference's
+        start for every initial image but a wFBP one)."""
         v = None if vol is None else np.ascontiguousarray(vol, dtype=np.float32)
-        check(lib().ctbb_gpu_recon_set_volume(self.handle, ssm.handle, ptr(v, C.c_float)))
+        check(lib().ctbb_gpu_recon_set_volume_estimate(self.handle, ssm.handle, ptr(v, C.c_float), int(estimate)))
 
     def volume(self) -> np.ndarray:
         out = np.empty(self.rp.shape, np.float32)
@@ -434,10 +437,13 @@ def icd_iteration(rp: ReconParams, data: CtData, ctx: Context | None = None,
     ctx = ctx or data.system_matrix.ctx
     rc = Recon(rp, data.slice_indices, ctx)
     try:
+        o = opts or icd_opts(mode=ICD_SEQUENTIAL)
         rc.set_raw(data.raw)
-        rc.set_volume(data.system_matrix, data.recon_volume)
-        st = rc.iterate(data.system_matrix, int(n_iter if n_iter is not None else rp.geom.num_iterations),
-                        opts or icd_opts(mode=ICD_SEQUENTIAL))
+        # icd_iteration.cpp:47-63: in parity mode the estimate is zero unless
+        # the start is a wFBP image (see ctbb_gpu_recon_set_volume_estimate).
+        est = ESTIMATE_ZERO if (o.mode == ICD_SEQUENTIAL and not rp.geom.wfbp_initialize) else ESTIMATE_FORWARD
+        rc.set_volume(data.system_matrix, data.recon_volume, est)
+        st = rc.iterate(data.system_matrix, int(n_iter if n_iter is not None else rp.geom.num_iterations), o)
         data.recon_volume = rc.volume()
         data.extra["volume_f64"] = rc.volume_f64()
     finally:

@@ -23,6 +23,8 @@ PENALTY_QUADRATIC, PENALTY_EDGE_PRESERVING = 0, 1
 SSM_FP32, SSM_FP16, SSM_BOTH = 1, 2, 3
 ICD_SEQUENTIAL, ICD_GROUPED = 0, 1
 ROTATE_FIXED2ROTATING, ROTATE_ROTATING2FIXED = 1, -1
+ESTIMATE_ZERO, ESTIMATE_FORWARD = 0, 1
+CNN_ENGINE_MMA_SYNC, CNN_ENGINE_TCGEN05 = 0, 1
 
 
 class CtbbError(RuntimeError):
@@ -182,6 +184,8 @@ PROTOTYPES = {
     "ctbb_gpu_recon_autotune": (_I, [_P, _P, C.POINTER(IcdOpts), _I, C.POINTER(IcdOpts), C.POINTER(TuneReport)]),
     "ctbb_gpu_recon_set_priority": (_I, [_P, C.POINTER(IcdOpts), _D]),
     "ctbb_gpu_penalty_steps": (_I, [_P, _I, _D, _D, _U, _PD, _PD, _PF, _PD]),
+    "ctbb_gpu_recon_set_volume_estimate": (_I, [_P, _P, _PF, _I]),
+    "ctbb_cnn_set_engine": (_I, [_P, _I]),
 }
 
 _lib = None

@@ -28,7 +28,8 @@ HOSTCXX = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 EXACT_CU = {"ssm.cu", "icd_seq.cu", "rotate.cu"}
-CU_SOURCES = ["ctx.cu", "ssm.cu", "rotate.cu", "recon.cu", "icd_seq.cu", "icd_grouped.cu", "cnn.cu", "tune.cu"]
+CU_SOURCES = ["ctx.cu", "ssm.cu", "rotate.cu", "recon.cu", "icd_seq.cu", "icd_grouped.cu", "cnn.cu", "cnn_tc.cu",
+              "tune.cu"]
 CPP_SOURCES = ["host_setup.cpp"]
 HEADERS = ["common.h", "gpu_internal.h", "phantom.h"]
 

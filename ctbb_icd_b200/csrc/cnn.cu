@@ -561,6 +561,9 @@ struct ctbb_cnn {
     uint64_t* d_offs = nullptr;
     __nv_bfloat16 *d_wf = nullptr, *d_wb = nullptr;
     bool weights_dirty = true;
+    // C -> C convolutions: CTBB_CNN_ENGINE_TCGEN05 (cnn_tc.cu) or
+    // CTBB_CNN_ENGINE_MMA_SYNC (conv_mid_kernel below).
+    int engine = CTBB_CNN_ENGINE_TCGEN05;
     // Activation workspace, grown on demand: a_0..a_B, h_0..h_{B-1}, two
     // gradient buffers and du.
     uint64_t cap = 0;
@@ -623,10 +626,24 @@ ctbb_status prep_weights(ctbb_cnn* c) {
 
 ctbb_status conv_mid(ctbb_cnn* c, const Dims& d, const __nv_bfloat16* in, const __nv_bfloat16* wt, const float* bias,
                      const __nv_bfloat16* residual, const __nv_bfloat16* mask, int relu, __nv_bfloat16* out) {
+    if (c->engine == CTBB_CNN_ENGINE_TCGEN05)
+        return conv_mid_tc(c->ctx, d.nx, d.ny, d.nz, in, wt, bias, residual, mask, relu, out, c->ctx->d_flags + 1);
     CTBB_TRY(configure_kernels(c->ctx->device));
     const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>(d.n_tiles, (uint64_t)c->ctx->sm_count * 2));
     conv_mid_kernel<<<grid, 256, kMidSmem, c->ctx->stream>>>(d, in, wt, bias, residual, mask, relu, out);
     CTBB_CUDA(cudaGetLastError());
+    return CTBB_OK;
+}
+
+// After a synchronised call: a tensor-core convolution whose mbarrier wait
+// ran out leaves 1 in the context's error flag 1 (cnn_tc.cu).
+ctbb_status check_conv_flag(ctbb_cnn* c) {
+    int h = 0;
+    CTBB_CUDA(cudaMemcpy(&h, c->ctx->d_flags + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (h) {
+        CTBB_CUDA(cudaMemset(c->ctx->d_flags + 1, 0, sizeof(int)));
+        return fail(CTBB_ERR_TIMEOUT, "tensor-core convolution: a wait for its loads or products expired");
+    }
     return CTBB_OK;
 }
 
@@ -808,6 +825,15 @@ extern "C" ctbb_status ctbb_cnn_forward(ctbb_cnn* c, const float* x_dev, int32_t
     const uint64_t n = (uint64_t)nx * ny * nz;
     CTBB_CUDA(cudaMemcpyAsync(out_dev, c->d_out, n * sizeof(float), cudaMemcpyDeviceToDevice, c->ctx->stream));
     CTBB_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    return check_conv_flag(c);
+}
+
+extern "C" ctbb_status ctbb_cnn_set_engine(ctbb_cnn* c, int32_t engine) {
+    clear_error();
+    if (!c) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (engine != CTBB_CNN_ENGINE_TCGEN05 && engine != CTBB_CNN_ENGINE_MMA_SYNC)
+        return fail(CTBB_ERR_INVALID_ARG, "unknown convolution engine %d", engine);
+    c->engine = engine;
     return CTBB_OK;
 }
 
@@ -866,6 +892,7 @@ extern "C" ctbb_status ctbb_cnn_accumulate_gradient(ctbb_cnn* c, const float* x_
                                                          c->d_g + c->off_win);
     CTBB_CUDA(cudaGetLastError());
     CTBB_CUDA(cudaStreamSynchronize(st));
+    CTBB_TRY(check_conv_flag(c));
     if (loss) *loss = L;
     return CTBB_OK;
 }
@@ -922,5 +949,7 @@ ctbb_status apply_correction(ctbb_ctx* ctx, uint64_t n, float* x_dev, const floa
 }
 
 ctbb_ctx* cnn_ctx(const ctbb_cnn* c) { return c->ctx; }
+
+ctbb_status cnn_check_flag(ctbb_cnn* c) { return check_conv_flag(c); }
 
 }  // namespace ctbb

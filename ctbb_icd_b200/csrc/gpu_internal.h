@@ -2,6 +2,7 @@
 // internal launch functions shared between translation units.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -92,6 +93,9 @@ struct ctbb_recon {
     uint32_t* d_prio_order = nullptr;
     uint64_t n_prio_order = 0;
     int prio_P = 0;
+    // Grouped iteration captured in a CUDA graph, and the launch it encodes.
+    cudaGraphExec_t icd_graph = nullptr;
+    std::vector<unsigned char> icd_graph_key;
 };
 
 struct ctbb_cnn;
@@ -130,9 +134,15 @@ ctbb_status inrange_entries(ctbb_recon* rc, const ctbb_ssm* ssm, double* out);
 ctbb_status rotate_volume(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tube_angles_deg,
                           const uint64_t* slice_indices, const float* d_in, float* d_out, int direction);
 
+// cnn_tc.cu
+ctbb_status conv_mid_tc(ctbb_ctx* ctx, int nx, int ny, int nz, const __nv_bfloat16* in, const __nv_bfloat16* wt,
+                        const float* bias, const __nv_bfloat16* residual, const __nv_bfloat16* mask, int relu,
+                        __nv_bfloat16* out, int* err);
+
 // cnn.cu
 ctbb_status cnn_predict_correction(ctbb_cnn* c, const float* x_dev, int nx, int ny, int nz, float* d_dev);
 ctbb_status apply_correction(ctbb_ctx* ctx, uint64_t n, float* x_dev, const float* d_dev, float* prio_dev);
 ctbb_ctx* cnn_ctx(const ctbb_cnn* c);
+ctbb_status cnn_check_flag(ctbb_cnn* c);
 
 }  // namespace ctbb

@@ -965,22 +965,40 @@ ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float
     return CTBB_OK;
 }
 
+// prepare: only raise the kernel's dynamic shared-memory limit (done before
+// a stream capture, outside it); otherwise launch on `st`.
 template <class WT, int U, int NW>
 ctbb_status launch_staged(const GParams& P, const uint32_t* order, const ctbb_ssm* ssm, const WT* w, ctbb_recon* rc,
-                          uint64_t in_flight, unsigned long long* stats) {
+                          uint64_t in_flight, unsigned long long* stats, cudaStream_t st, bool prepare) {
     ctbb_ctx* ctx = rc->ctx;
     const int cap = stage_capacity(ctx, NW, (int)sizeof(WT));
     const size_t smem = (size_t)NW * (size_t)cap * (4 + sizeof(WT));
-    CTBB_CUDA(cudaFuncSetAttribute(icd_staged_kernel<WT, U, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
+    if (prepare) {
+        CTBB_CUDA(cudaFuncSetAttribute(icd_staged_kernel<WT, U, NW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
+        return CTBB_OK;
+    }
     // One CTA per SM is resident (the stage takes the SM's shared memory);
     // a persistent grid larger than that would only add idle CTAs.
     const int blocks = (int)std::max<uint64_t>(1, std::min<uint64_t>((in_flight + NW - 1) / NW, ctx->sm_count));
-    icd_staged_kernel<WT, U, NW><<<blocks, 32 * NW, smem, ctx->stream>>>(
-        P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx, w, rc->d_start, rc->d_e32, rc->d_x32, ctx->d_queue, cap,
-        stats);
+    icd_staged_kernel<WT, U, NW><<<blocks, 32 * NW, smem, st>>>(P, order, ssm->d_colptr, ssm->d_vptr, ssm->d_idx, w,
+                                                                rc->d_start, rc->d_e32, rc->d_x32, ctx->d_queue, cap,
+                                                                stats);
     return CTBB_OK;
 }
+
+// What a captured iteration depends on: a graph is reused while the key is
+// unchanged (byte comparison; the struct is zero-filled before use).
+struct GraphKey {
+    GParams P;
+    const void* order;
+    const void* w;
+    const void* idx;
+    const float* e;
+    const float* x;
+    uint64_t in_flight;
+    int stage, wpv, epl, h;
+};
 
 
 // Build (or reuse) the full visiting order for tile edge P_lat.
@@ -1064,74 +1082,129 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const int stage = o.stage_column;
     if (stage < 0 || stage > 2) return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0, 1 or 2 (got %d)", stage);
     if (stage && wpv != 1) return fail(CTBB_ERR_INVALID_ARG, "stage_column needs one warp per voxel update");
+    const int epl = o.entries_per_lane > 0 ? o.entries_per_lane : kU;
+    if (epl != 8 && epl != 16) return fail(CTBB_ERR_INVALID_ARG, "entries_per_lane must be 8 or 16 (got %d)", epl);
     ctbb_ctx* ctx = rc->ctx;
     cudaStream_t st = ctx->stream;
     unsigned long long* stats = ctx->d_queue + 2;
-    CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned long long), st));
-    cudaEvent_t e0, e1;
-    CTBB_CUDA(cudaEventCreate(&e0));
-    CTBB_CUDA(cudaEventCreate(&e1));
-    CTBB_CUDA(cudaEventRecord(e0, st));
     const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
     const bool h = wsel == CTBB_SSM_FP16;
     const int64_t* cp = ssm->d_colptr;
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
-    const int epl = o.entries_per_lane > 0 ? o.entries_per_lane : kU;
-    if (epl != 8 && epl != 16) return fail(CTBB_ERR_INVALID_ARG, "entries_per_lane must be 8 or 16 (got %d)", epl);
-    if (stage) {
-        // stage_column 1: 4 warps (updates) per CTA, 2: 8 (half the stage each).
-        if (stage == 1) {
+
+    // One iteration: reset the work queue and the scatter counters, then the
+    // persistent kernel (prepare: only the launch attributes, no work).
+    auto issue = [&](cudaStream_t s, bool prepare) -> ctbb_status {
+        if (!prepare) CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned long long), s));
+        if (stage) {
+            // stage_column 1: 4 warps (updates) per CTA, 2: 8 (half the stage each).
+            if (stage == 1) {
+                if (h)
+                    return (epl == 16 ? launch_staged<__half, 16, 4> : launch_staged<__half, 8, 4>)(
+                        P, order, ssm, ssm->d_w16, rc, in_flight, stats, s, prepare);
+                return (epl == 16 ? launch_staged<float, 16, 4> : launch_staged<float, 8, 4>)(
+                    P, order, ssm, ssm->d_w32, rc, in_flight, stats, s, prepare);
+            }
             if (h)
-                CTBB_TRY((epl == 16 ? launch_staged<__half, 16, 4> : launch_staged<__half, 8, 4>)(
-                    P, order, ssm, ssm->d_w16, rc, in_flight, stats));
-            else
-                CTBB_TRY((epl == 16 ? launch_staged<float, 16, 4> : launch_staged<float, 8, 4>)(
-                    P, order, ssm, ssm->d_w32, rc, in_flight, stats));
-        } else {
-            if (h)
-                CTBB_TRY((epl == 16 ? launch_staged<__half, 16, 8> : launch_staged<__half, 8, 8>)(
-                    P, order, ssm, ssm->d_w16, rc, in_flight, stats));
-            else
-                CTBB_TRY((epl == 16 ? launch_staged<float, 16, 8> : launch_staged<float, 8, 8>)(
-                    P, order, ssm, ssm->d_w32, rc, in_flight, stats));
+                return (epl == 16 ? launch_staged<__half, 16, 8> : launch_staged<__half, 8, 8>)(
+                    P, order, ssm, ssm->d_w16, rc, in_flight, stats, s, prepare);
+            return (epl == 16 ? launch_staged<float, 16, 8> : launch_staged<float, 8, 8>)(
+                P, order, ssm, ssm->d_w32, rc, in_flight, stats, s, prepare);
         }
-    } else if (wpv == 1) {
-        const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
-        if (epl == 16) {
-            if (h)
-                icd_grouped_kernel<__half, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                       rc->d_e32, rc->d_x32, ctx->d_queue, stats);
-            else
-                icd_grouped_kernel<float, 16><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+        if (prepare) return CTBB_OK;
+        if (wpv == 1) {
+            const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
+            if (epl == 16) {
+                if (h)
+                    icd_grouped_kernel<__half, 16><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                          rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+                else
+                    icd_grouped_kernel<float, 16><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                         rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            } else {
+                if (h)
+                    icd_grouped_kernel<__half, 8><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                         rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+                else
+                    icd_grouped_kernel<float, 8><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                        rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            }
         } else {
-            if (h)
-                icd_grouped_kernel<__half, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
-            else
-                icd_grouped_kernel<float, 8><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            const int blocks = (int)in_flight;
+            if (wpv == 8) {
+                if (h)
+                    icd_cta_kernel<__half, 8, 32><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                         rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+                else
+                    icd_cta_kernel<float, 8, 32><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                        rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            } else {
+                if (h)
+                    icd_cta_kernel<__half, 4, 32><<<blocks, 128, 0, s>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
+                                                                         rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+                else
+                    icd_cta_kernel<float, 4, 32><<<blocks, 128, 0, s>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
+                                                                        rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            }
         }
-    } else {
-        const int blocks = (int)in_flight;
-        if (wpv == 8) {
-            if (h)
-                icd_cta_kernel<__half, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
-            else
-                icd_cta_kernel<float, 8, 32><<<blocks, 256, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+        CTBB_CUDA(cudaGetLastError());
+        return CTBB_OK;
+    };
+
+    // The iteration is captured once in a CUDA graph per launch shape and
+    // replayed; a stream that cannot be captured (the legacy default stream)
+    // issues the same two operations directly.
+    GraphKey key;
+    memset(&key, 0, sizeof(key));
+    key.P = P;
+    key.order = order;
+    key.w = h ? (const void*)ssm->d_w16 : (const void*)ssm->d_w32;
+    key.idx = ix;
+    key.e = rc->d_e32;
+    key.x = rc->d_x32;
+    key.in_flight = in_flight;
+    key.stage = stage;
+    key.wpv = wpv;
+    key.epl = epl;
+    key.h = h;
+    const bool have = rc->icd_graph && rc->icd_graph_key.size() == sizeof(key) &&
+                      memcmp(rc->icd_graph_key.data(), &key, sizeof(key)) == 0;
+    if (!have) {
+        if (rc->icd_graph) cudaGraphExecDestroy(rc->icd_graph);
+        rc->icd_graph = nullptr;
+        rc->icd_graph_key.clear();
+        CTBB_TRY(issue(st, true));
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        CTBB_CUDA(cudaStreamIsCapturing(st, &cs));
+        if (st != nullptr && cs == cudaStreamCaptureStatusNone &&
+            cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+            const ctbb_status is = issue(st, false);
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(st, &g);
+            if (is != CTBB_OK || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return is != CTBB_OK ? is : fail(CTBB_ERR_CUDA, "ICD iteration capture: %s", cudaGetErrorString(ce));
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&rc->icd_graph, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) {
+                rc->icd_graph = nullptr;
+                return fail(CTBB_ERR_CUDA, "ICD iteration graph: %s", cudaGetErrorString(ie));
+            }
+            rc->icd_graph_key.assign((const unsigned char*)&key, (const unsigned char*)&key + sizeof(key));
         } else {
-            if (h)
-                icd_cta_kernel<__half, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w16, rc->d_start,
-                                                                      rc->d_e32, rc->d_x32, ctx->d_queue, stats);
-            else
-                icd_cta_kernel<float, 4, 32><<<blocks, 128, 0, st>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
-                                                                     rc->d_e32, rc->d_x32, ctx->d_queue, stats);
+            cudaGetLastError();  // a refused capture leaves no lasting error
         }
     }
-    CTBB_CUDA(cudaGetLastError());
+    cudaEvent_t e0, e1;
+    CTBB_CUDA(cudaEventCreate(&e0));
+    CTBB_CUDA(cudaEventCreate(&e1));
+    CTBB_CUDA(cudaEventRecord(e0, st));
+    if (rc->icd_graph)
+        CTBB_CUDA(cudaGraphLaunch(rc->icd_graph, st));
+    else
+        CTBB_TRY(issue(st, false));
     CTBB_CUDA(cudaEventRecord(e1, st));
     CTBB_CUDA(cudaEventSynchronize(e1));
     cudaEventElapsedTime(ms, e0, e1);

@@ -227,10 +227,15 @@ int main(int argc, char** argv) {
     ctbb_recon* rc = nullptr;
     die(ctbb_gpu_recon_create(ctx, &g, slice_indices.data(), &rc), "icd_iteration");
     die(ctbb_gpu_recon_set_raw(rc, raw.data()), "icd_iteration");
-    die(ctbb_gpu_recon_set_volume(rc, ssm, vol.data()), "icd_iteration");
     ctbb_icd_opts o;
     memset(&o, 0, sizeof(o));
     o.mode = fl.sequential ? CTBB_ICD_SEQUENTIAL : CTBB_ICD_GROUPED;
+    // icd_iteration.cpp:47-63: the reference forward-projects the start only
+    // for a wFBP image; in parity mode an initial_recon_path image starts
+    // against a zero estimate as it does there.
+    const int32_t est =
+        (fl.sequential && !g.wfbp_initialize) ? CTBB_ESTIMATE_ZERO : CTBB_ESTIMATE_FORWARD;
+    die(ctbb_gpu_recon_set_volume_estimate(rc, ssm, vol.data(), est), "icd_iteration");
     o.weights = wfmt;
     o.refresh_every = fl.sequential ? 0 : 10;
     const std::string dump_dir = std::string(s.output_dir) + "/reconstructions";

@@ -297,6 +297,7 @@ extern "C" void ctbb_gpu_recon_free(ctbb_recon* rc) {
     cudaFree(rc->d_order);
     cudaFree(rc->d_prio);
     cudaFree(rc->d_prio_order);
+    if (rc->icd_graph) cudaGraphExecDestroy(rc->icd_graph);
     ctx_release(rc->ctx);
     delete rc;
 }
@@ -332,9 +333,12 @@ extern "C" ctbb_status ctbb_gpu_recon_get_raw(ctbb_recon* rc, float* raw_host) {
     return CTBB_OK;
 }
 
-extern "C" ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host) {
+extern "C" ctbb_status ctbb_gpu_recon_set_volume_estimate(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host,
+                                                          int32_t estimate) {
     clear_error();
     if (!rc || !ssm) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    if (estimate != CTBB_ESTIMATE_ZERO && estimate != CTBB_ESTIMATE_FORWARD)
+        return fail(CTBB_ERR_INVALID_ARG, "estimate must be CTBB_ESTIMATE_ZERO or CTBB_ESTIMATE_FORWARD");
     CTBB_TRY(check_pair(rc, ssm));
     CTBB_CUDA(cudaSetDevice(rc->ctx->device));
     cudaStream_t st = rc->ctx->stream;
@@ -342,7 +346,10 @@ extern "C" ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm*
         CTBB_CUDA(cudaMemcpyAsync(rc->d_x32, vol_host, rc->nvox * sizeof(float), cudaMemcpyHostToDevice, st));
         f32_to_f64_kernel<<<grid_for(rc->ctx, rc->nvox, 256), 256, 0, st>>>(rc->d_x32, rc->d_x64, rc->nvox);
         CTBB_CUDA(cudaGetLastError());
-        CTBB_TRY(forward_project_f64(rc, ssm, false, rc->d_est64));
+        if (estimate == CTBB_ESTIMATE_FORWARD)
+            CTBB_TRY(forward_project_f64(rc, ssm, false, rc->d_est64));
+        else  // icd_iteration.cpp:47, 63: the estimate stays zero unless a wFBP start forward-projects it
+            CTBB_CUDA(cudaMemsetAsync(rc->d_est64, 0, rc->data_size * sizeof(double), st));
     } else {
         CTBB_CUDA(cudaMemsetAsync(rc->d_x32, 0, rc->nvox * sizeof(float), st));
         CTBB_CUDA(cudaMemsetAsync(rc->d_x64, 0, rc->nvox * sizeof(double), st));
@@ -354,6 +361,10 @@ extern "C" ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm*
     CTBB_CUDA(cudaStreamSynchronize(st));
     rc->rep = 0;  // both representations are current; sequential is the canonical one
     return CTBB_OK;
+}
+
+extern "C" ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host) {
+    return ctbb_gpu_recon_set_volume_estimate(rc, ssm, vol_host, CTBB_ESTIMATE_FORWARD);
 }
 
 extern "C" ctbb_status ctbb_gpu_recon_get_volume(ctbb_recon* rc, float* vol_host) {
@@ -461,8 +472,15 @@ extern "C" ctbb_status ctbb_gpu_recon_iterate(ctbb_recon* rc, const ctbb_ssm* ss
         s.entries += entries;
         s.voxel_updates += upd;
         if (opts->compute_cost || opts->stop_rel_change > 0.0) {
+            // Exact FP64 cost: in grouped mode A x is recomputed in FP64 (not
+            // the incrementally updated FP32 e), and e is refreshed from it.
             double c = 0.0;
-            CTBB_TRY(cost_f64(rc, ssm, false, &c));
+            CTBB_TRY(cost_f64(rc, ssm, true, &c));
+            if (rc->rep == 1) {
+                residual_kernel<<<grid_for(rc->ctx, rc->data_size, 256), 256, 0, rc->ctx->stream>>>(
+                    rc->d_raw, rc->d_est64, rc->d_e32, rc->data_size);
+                CTBB_CUDA(cudaGetLastError());
+            }
             s.cost = c;
             if (!isnan(prev_cost)) {
                 s.rel_change = fabs(prev_cost - c) / fmax(fabs(c), 1e-300);
@@ -492,7 +510,13 @@ extern "C" ctbb_status ctbb_gpu_icd(ctbb_ctx* ctx, const ctbb_ssm* ssm, const ct
     ctbb_recon* rc = nullptr;
     CTBB_TRY(ctbb_gpu_recon_create(ctx, geom, slice_indices, &rc));
     ctbb_status st = ctbb_gpu_recon_set_raw(rc, raw);
-    if (st == CTBB_OK) st = ctbb_gpu_recon_set_volume(rc, ssm, recon_volume);
+    // Sequential (parity) mode starts like icd_iteration.cpp:47-63: the
+    // sinogram estimate is forward-projected only for a wFBP start, so an
+    // initial image loaded from initial_recon_path starts with y_hat = 0.
+    // Grouped mode always starts from a consistent e = y - A x.
+    const int32_t est = (o.mode == CTBB_ICD_SEQUENTIAL && !geom->wfbp_initialize) ? CTBB_ESTIMATE_ZERO
+                                                                                  : CTBB_ESTIMATE_FORWARD;
+    if (st == CTBB_OK) st = ctbb_gpu_recon_set_volume_estimate(rc, ssm, recon_volume, est);
     if (st == CTBB_OK) st = ctbb_gpu_recon_iterate(rc, ssm, &o, (int32_t)geom->num_iterations, stats);
     if (st == CTBB_OK) st = ctbb_gpu_recon_get_volume(rc, recon_volume);
     ctbb_gpu_recon_free(rc);
@@ -527,6 +551,7 @@ extern "C" ctbb_status ctbb_gpu_recon_warm_start(ctbb_recon* rc, const ctbb_ssm*
                            CTBB_ROTATE_FIXED2ROTATING);
     if (st == CTBB_OK) st = apply_correction(rc->ctx, n, rc->d_x32, d_a, rc->d_prio);
     if (st == CTBB_OK) st = ctbb_gpu_recon_refresh_residual(rc, ssm);
+    if (st == CTBB_OK) st = cnn_check_flag(cnn);
     cudaFree(d_a);
     cudaFree(d_b);
     cudaFree(rc->d_prio_order);

@@ -272,8 +272,10 @@ typedef struct ctbb_icd_opts {
                                  capped at one cell rank of the visiting order      */
     int32_t lattice;          /* grouped: tile edge of the visiting order (0: derived from
                                  the warps in flight)                              */
-    int32_t compute_cost;     /* evaluate the FP64 cost after each iteration      */
-    double stop_rel_change;   /* stop when |dcost|/cost < this (0: fixed count)   */
+    int32_t compute_cost;     /* evaluate the exact FP64 cost after each iteration
+                                 (grouped mode: FP64 A x recomputed, e refreshed) */
+    double stop_rel_change;   /* stop when |dcost|/cost < this, exact FP64 costs
+                                 of consecutive iterations (0: fixed count)        */
     double relax;             /* grouped: step scale omega in (0, 2) (0: 1.0)     */
     int32_t priority;         /* grouped: visit only the priority subset built by
                                  ctbb_gpu_recon_set_priority (0: every voxel)     */
@@ -332,6 +334,16 @@ ctbb_status ctbb_gpu_recon_get_raw(ctbb_recon* rc, float* raw_host);
 float* ctbb_gpu_recon_raw_device(ctbb_recon* rc);
 /* Initial image (host, float [nz][ny][nx]); NULL -> zeros. Resets e = y - Ax. */
 ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host);
+/* Same, choosing the starting sinogram estimate: CTBB_ESTIMATE_FORWARD
+ * y_hat = A x0 (what ctbb_gpu_recon_set_volume does), or CTBB_ESTIMATE_ZERO
+ * y_hat = 0 whatever x0 is, which is what the reference's icd_iteration does
+ * for every start but a wFBP one (icd_iteration.cpp:47, 63): with an image
+ * from initial_recon_path its first iteration measures the data against a
+ * zero projection. ctbb_gpu_icd uses ZERO in sequential (parity) mode unless
+ * geom->wfbp_initialize is set, and FORWARD in grouped mode. */
+enum { CTBB_ESTIMATE_ZERO = 0, CTBB_ESTIMATE_FORWARD = 1 };
+ctbb_status ctbb_gpu_recon_set_volume_estimate(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host,
+                                               int32_t estimate);
 ctbb_status ctbb_gpu_recon_get_volume(ctbb_recon* rc, float* vol_host);
 ctbb_status ctbb_gpu_recon_get_volume_f64(ctbb_recon* rc, double* vol_host);
 /* Run n_iter ICD iterations. */
@@ -471,6 +483,12 @@ ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* ssm, const c
 typedef struct ctbb_cnn ctbb_cnn;
 ctbb_status ctbb_cnn_create(ctbb_ctx* ctx, int32_t blocks, uint64_t seed, ctbb_cnn** out);
 void ctbb_cnn_free(ctbb_cnn* cnn);
+/* Tensor-core path of the 32 -> 32 convolutions (forward and backward-data):
+ * TCGEN05 (default) = tcgen05.mma with a TMEM accumulator and TMA-staged
+ * operands; MMA_SYNC = the warp-level mma.sync kernel, kept as a cross-check.
+ * A tcgen05 wait that runs out makes the call return CTBB_ERR_TIMEOUT. */
+enum { CTBB_CNN_ENGINE_MMA_SYNC = 0, CTBB_CNN_ENGINE_TCGEN05 = 1 };
+ctbb_status ctbb_cnn_set_engine(ctbb_cnn* cnn, int32_t engine);
 uint64_t ctbb_cnn_num_params(const ctbb_cnn* cnn);
 ctbb_status ctbb_cnn_get_params(ctbb_cnn* cnn, float* params_host, uint64_t n);
 ctbb_status ctbb_cnn_set_params(ctbb_cnn* cnn, const float* params_host, uint64_t n);

@@ -238,3 +238,31 @@ def test_trained_warm_start_beats_plain_icd(ctx):
     assert c_learned < c_plain, (c_learned, c_plain)
     assert scan.error_hu(x_learned, x_long) < scan.error_hu(x_plain, x_long)
     net.free()
+
+
+@pytest.mark.parametrize("shape", [(3, 8, 16), (5, 37, 150), (2, 130, 257)])
+def test_tcgen05_convolutions_match_mma_sync(ctx, shape):
+    """The tcgen05 path (TMA-staged halo, 54 tcgen05.mma per 128-voxel line,
+    TMEM accumulator) against the warp-level mma.sync kernel on ragged
+    volumes (x extents that are not multiples of the 128-voxel tile, edges
+    in every direction): same BF16 operands, FP32 accumulation in a different
+    order, so outputs and gradients agree to BF16 rounding of the
+    activations."""
+    torch = _torch()
+    net = L.WarmStartNet(ctx, 2, seed=3)
+    x = torch.from_numpy(_phantom(shape, 11).astype(np.float32)).cuda()
+    xc = (x + 0.002 * torch.randn_like(x)).contiguous()
+    out = {}
+    grads = {}
+    for engine in (C.CNN_ENGINE_MMA_SYNC, C.CNN_ENGINE_TCGEN05):
+        net.set_engine(engine)
+        out[engine] = net.forward(x).cpu().numpy()
+        net.zero_gradient()
+        net.accumulate_gradient(x, xc)
+        grads[engine] = net.gradient()
+    a, b = out[C.CNN_ENGINE_MMA_SYNC], out[C.CNN_ENGINE_TCGEN05]
+    assert np.isfinite(b).all()
+    assert np.linalg.norm(a - b) <= 1e-2 * np.linalg.norm(a), np.linalg.norm(a - b) / np.linalg.norm(a)
+    ga, gb = grads[C.CNN_ENGINE_MMA_SYNC], grads[C.CNN_ENGINE_TCGEN05]
+    assert np.linalg.norm(ga - gb) <= 2e-2 * np.linalg.norm(ga), np.linalg.norm(ga - gb) / np.linalg.norm(ga)
+    net.free()

@@ -297,3 +297,72 @@ def test_grouped_edge_preserving_reaches_converged_cost(ctx, converged_small_ffs
     assert rmse_hu <= 0.5, rmse_hu
     assert abs(costs[-1] - cost_ref) <= 1e-6 * abs(cost_ref), (costs[-1], cost_ref)
     rc.free()
+
+
+def test_initial_recon_path_start_matches_reference(golden, ctx, tmp_path):
+    """A start from initial_recon_path (initialize_recon_volume.cpp:57-76)
+    without wFBP: the reference keeps its sinogram estimate at zero
+    (icd_iteration.cpp:47, 63); the parity mode does the same, and its first
+    two iterations match the reference program's dumps."""
+    from oracle import reference_run as R
+
+    d = str(tmp_path)
+    x0 = (golden.iterations[1] * 0.5).astype(np.float32)  # a non-zero start
+    x0_path = os.path.join(d, "x0.img")
+    x0.tofile(x0_path)
+    text = open(golden.prm_path).read().replace(golden.dir, d)
+    text = "\n".join(l for l in text.splitlines() if not l.startswith(("num_iterations", "initial_recon_path")))
+    text += f"\nnum_iterations: 2\ninitial_recon_path: {x0_path}\n"
+    prm_path = os.path.join(d, "start.prm")
+    with open(prm_path, "w") as f:
+        f.write(text)
+    golden.raw.tofile(os.path.join(d, f"{golden.name}.bin"))
+    rc_ref, stamps = R.run("O2", prm_path, d, threads=2)
+    assert rc_ref == 0, stamps[-5:]
+
+    rp = C.configure_recon_params(prm_path)
+    data = C.load_raw(rp)
+    C.initialize_recon_volume(rp, data)
+    assert np.array_equal(data.recon_volume, x0)
+    ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, data.recon_volume, C.ESTIMATE_ZERO)
+    for it in (1, 2):
+        rc.iterate(ssm, 1, C.icd_opts(mode=C.ICD_SEQUENTIAL))
+        ref = np.fromfile(os.path.join(d, "reconstructions", f"iteration{it}.rcn"), np.float64).reshape(rp.shape)
+        x = rc.volume_f64()
+        rel = np.linalg.norm(x - ref) / np.linalg.norm(ref)
+        assert rel < 1e-12, (golden.name, it, rel)
+    # The stage functions apply the same start in sequential mode.
+    data2 = C.load_raw(rp)
+    C.initialize_recon_volume(rp, data2)
+    data2.system_matrix = ssm
+    C.icd_iteration(rp, data2, ctx)
+    assert np.allclose(data2.extra["volume_f64"], ref, rtol=1e-12, atol=1e-15)
+    rc.free()
+
+
+def test_stop_rel_change_uses_exact_cost(ctx, converged_cfg1_small):
+    """The stopping rule compares exact FP64 costs (A x recomputed in FP64 in
+    grouped mode): it stops once the relative change falls below the
+    threshold, and the cost it reports is the oracle's FP64 cost of the image
+    it returns."""
+    rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
+    rc = C.Recon(rp, data.slice_indices, ctx)
+    rc.set_raw(data.raw)
+    rc.set_volume(ssm, None)
+    st = rc.iterate(ssm, 200, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, stop_rel_change=1e-5))
+    assert 1 < st.iterations < 200, st.iterations
+    assert st.rel_change < 1e-5
+    csr = O.Csr(*[np.asarray(a) for a in _ssm_arrays(ssm, rp)])
+    oracle_cost, _, _ = O.port_cost(rp, data.slice_indices, data.raw, csr, rc.volume_f64())
+    assert abs(st.cost - oracle_cost) <= 1e-9 * abs(oracle_cost), (st.cost, oracle_cost)
+    rc.free()
+
+
+def _ssm_arrays(ssm, rp):
+    ncol = int(rp.geom.nx * rp.geom.ny)
+    cols = [ssm.column(c) for c in range(ncol)]
+    colptr = np.concatenate([[0], np.cumsum([c[0].size for c in cols])]).astype(np.int64)
+    return colptr, np.concatenate([c[0] for c in cols]), np.concatenate([c[1] for c in cols])
