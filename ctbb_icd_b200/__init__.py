@@ -314,6 +314,11 @@ class Recon:
         v = None if vol is None else np.ascontiguousarray(vol, dtype=np.float32)
         check(lib().ctbb_gpu_recon_set_volume_estimate(self.handle, ssm.handle, ptr(v, C.c_float), int(estimate)))
 
+    def set_volume_upsampled(self, ssm: Ssm, coarse: "Recon"):
+        """Start from `coarse`'s image (half the in-plane size, same scan,
+        slices and FOV) upsampled 2x in-plane; e = y - A x refreshed in FP64."""
+        check(lib().ctbb_gpu_recon_set_volume_upsampled(self.handle, ssm.handle, coarse.handle))
+
     def volume(self) -> np.ndarray:
         out = np.empty(self.rp.shape, np.float32)
         check(lib().ctbb_gpu_recon_get_volume(self.handle, ptr(out, C.c_float)))

@@ -186,6 +186,7 @@ PROTOTYPES = {
     "ctbb_gpu_penalty_steps": (_I, [_P, _I, _D, _D, _U, _PD, _PD, _PF, _PD]),
     "ctbb_gpu_recon_set_volume_estimate": (_I, [_P, _P, _PF, _I]),
     "ctbb_cnn_set_engine": (_I, [_P, _I]),
+    "ctbb_gpu_recon_set_volume_upsampled": (_I, [_P, _P, _P]),
 }
 
 _lib = None

@@ -63,6 +63,27 @@ __global__ void f64_to_f32_kernel(const double* __restrict__ a, float* __restric
         b[i] = (float)a[i];
 }
 
+// In-plane 2x bilinear upsampling of a coarse image onto a grid with the same
+// field of view and slices and half the voxel size: fine voxel (i, j) sits
+// at coarse coordinates (i/2 - 1/4, j/2 - 1/4) (both grids centred, voxel
+// centres at (index - (n-1)/2) * size); clamped at the edges.
+__global__ void upsample2_kernel(const float* __restrict__ xc, int ncx, int ncy, int nz, float* __restrict__ xf) {
+    const int nfx = 2 * ncx, nfy = 2 * ncy;
+    const uint64_t n = (uint64_t)nfx * nfy * nz;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(t % nfx), j = (int)((t / nfx) % nfy), k = (int)(t / ((uint64_t)nfx * nfy));
+        const float u = fminf(fmaxf(0.5f * i - 0.25f, 0.f), (float)(ncx - 1));
+        const float v = fminf(fmaxf(0.5f * j - 0.25f, 0.f), (float)(ncy - 1));
+        const int i0 = min((int)u, max(ncx - 2, 0)), j0 = min((int)v, max(ncy - 2, 0));
+        const int i1 = min(i0 + 1, ncx - 1), j1 = min(j0 + 1, ncy - 1);
+        const float a = u - (float)i0, b = v - (float)j0;
+        const float* s = xc + (uint64_t)k * ncx * ncy;
+        const float top = (1.f - a) * s[(uint64_t)j0 * ncx + i0] + a * s[(uint64_t)j0 * ncx + i1];
+        const float bot = (1.f - a) * s[(uint64_t)j1 * ncx + i0] + a * s[(uint64_t)j1 * ncx + i1];
+        xf[t] = (1.f - b) * top + b * bot;
+    }
+}
+
 __global__ void f32_to_f64_kernel(const float* __restrict__ a, double* __restrict__ b, uint64_t n) {
     for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
         b[i] = (double)a[i];
@@ -360,6 +381,41 @@ extern "C" ctbb_status ctbb_gpu_recon_set_volume_estimate(ctbb_recon* rc, const 
     CTBB_CUDA(cudaGetLastError());
     CTBB_CUDA(cudaStreamSynchronize(st));
     rc->rep = 0;  // both representations are current; sequential is the canonical one
+    return CTBB_OK;
+}
+
+extern "C" ctbb_status ctbb_gpu_recon_set_volume_upsampled(ctbb_recon* fine, const ctbb_ssm* fine_ssm,
+                                                            ctbb_recon* coarse) {
+    clear_error();
+    if (!fine || !fine_ssm || !coarse) return fail(CTBB_ERR_INVALID_ARG, "null argument");
+    CTBB_TRY(check_pair(fine, fine_ssm));
+    const ctbb_geom_c& gf = fine->geom;
+    const ctbb_geom_c& gc = coarse->geom;
+    if (fine->ctx != coarse->ctx) return fail(CTBB_ERR_INVALID_ARG, "reconstructions on different contexts");
+    if (gf.num_voxels_x != 2 * gc.num_voxels_x || gf.num_voxels_y != 2 * gc.num_voxels_y ||
+        gf.num_voxels_z != gc.num_voxels_z || gf.recon_fov != gc.recon_fov || gf.Readings != gc.Readings ||
+        fine->slice_indices != coarse->slice_indices)
+        return fail(CTBB_ERR_INVALID_ARG,
+                    "the fine grid must have twice the coarse grid's in-plane size, the same field of view, "
+                    "scan and slices");
+    CTBB_CUDA(cudaSetDevice(fine->ctx->device));
+    cudaStream_t st = fine->ctx->stream;
+    if (coarse->rep == 0) {
+        f64_to_f32_kernel<<<grid_for(coarse->ctx, coarse->nvox, 256), 256, 0, st>>>(coarse->d_x64, coarse->d_x32,
+                                                                                    coarse->nvox);
+        CTBB_CUDA(cudaGetLastError());
+    }
+    upsample2_kernel<<<grid_for(fine->ctx, fine->nvox, 256), 256, 0, st>>>(
+        coarse->d_x32, (int)gc.num_voxels_x, (int)gc.num_voxels_y, (int)gc.num_voxels_z, fine->d_x32);
+    CTBB_CUDA(cudaGetLastError());
+    f32_to_f64_kernel<<<grid_for(fine->ctx, fine->nvox, 256), 256, 0, st>>>(fine->d_x32, fine->d_x64, fine->nvox);
+    CTBB_CUDA(cudaGetLastError());
+    CTBB_TRY(forward_project_f64(fine, fine_ssm, false, fine->d_est64));
+    residual_kernel<<<grid_for(fine->ctx, fine->data_size, 256), 256, 0, st>>>(fine->d_raw, fine->d_est64,
+                                                                               fine->d_e32, fine->data_size);
+    CTBB_CUDA(cudaGetLastError());
+    CTBB_CUDA(cudaStreamSynchronize(st));
+    fine->rep = 0;
     return CTBB_OK;
 }
 

@@ -1,12 +1,16 @@
 """Time to a given accuracy: plain grouped ICD vs the learned warm start.
 
-    python -m ctbb_icd_b200.eval_warm_start [--workload cfg2_slab] [--seed 950]
+    python -m ctbb_icd_b200.eval_warm_start [--workload cfg2] [--seed 950]
         [--weights ctbb_icd_b200/weights/warm_start.npz] [--tol 0.5] [--max-iter 400]
         [--ref-iter 1200] [--autotune] [--out result.json]
 
 Both arms start from the zero image (initialize_recon_volume's default) on the
 same scan and run the same grouped-ICD settings (autotuned once with
---autotune). The reference image is the unique minimiser of the convex cost,
+--autotune). On a scan twice the network's training grid in-plane (cfg2,
+512 x 512, for the 256 x 256 training grid) the learned arm starts on the
+scan's half-size grid (learned.warm_start_coarse); its matrix build is timed
+and reported apart from the reconstruction time, like the full-size matrix
+both arms use. The reference image is the unique minimiser of the convex cost,
 approached by the learned path followed by --ref-iter further iterations; the
 run reports how far that reference still moved over its last ten
 iterations. Errors are RMSE in HU inside the object support on the interior
@@ -46,10 +50,17 @@ def main(argv=None):
 
     torch.cuda.set_device(0)
     ctx = C.Context(0)
-    name = args.workload or L.TRAIN_WORKLOAD
+    name = args.workload or "cfg2"
     log = lambda m: print(m, file=sys.stderr, flush=True)  # noqa: E731
     net = L.WarmStartNet.load(ctx, args.weights or L.WEIGHTS_PATH)
     scan = L.make_scan(ctx, name, args.seed)
+    coarse, coarse_setup_s = None, None
+    train_nx = L.workload_shape(L.TRAIN_WORKLOAD)[2]
+    if int(scan.rp.geom.nx) == 2 * train_nx:
+        t0 = time.time()
+        coarse = L.make_scan(ctx, L.coarse_workload(name), args.seed, raw_from=scan)
+        coarse_setup_s = time.time() - t0
+        log(f"half-size grid {coarse.rp.shape}: matrix and setup {coarse_setup_s:.2f} s")
     opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_per_voxel=args.wpv)
     tune = None
     if args.autotune:
@@ -61,9 +72,13 @@ def main(argv=None):
 
     # Reference: learned start, then ref_iter iterations with FP64 refreshes.
     t0 = time.time()
-    scan.rc.set_volume(scan.ssm, None)
-    scan.rc.iterate(scan.ssm, args.n_early, net.early_opts(scan.rc, opts))
-    scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
+    copts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
+    if coarse is not None:
+        L.warm_start_coarse(scan, coarse, net, args.n_early, copts)
+    else:
+        scan.rc.set_volume(scan.ssm, None)
+        scan.rc.iterate(scan.ssm, args.n_early, net.early_opts(scan.rc, opts))
+        scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
     done = 0
     while done < args.ref_iter:
         n = min(50, args.ref_iter - done)
@@ -85,7 +100,7 @@ def main(argv=None):
     log(f"plain: {plain['seconds']:.2f} s, {plain['iterations']} iterations, reached {plain['reached']}")
     learned = L.time_to_tolerance(scan, x_ref, opts, tol_hu=args.tol, max_iter=args.max_iter, net=net,
                                   n_early=args.n_early, prio_fraction=args.prio_fraction,
-                                  prio_passes=args.prio_passes)
+                                  prio_passes=args.prio_passes, coarse=coarse, coarse_opts=copts)
     log(f"learned: {learned['seconds']:.2f} s, {learned['iterations']} iterations, reached {learned['reached']}")
 
     ladder = [1000.0, 500.0, 200.0, 100.0, 50.0, 25.0, 10.0, 5.0, 1.0, args.tol]
@@ -115,6 +130,9 @@ def main(argv=None):
         "opts": {"warps_per_voxel": max(1, opts.warps_per_voxel), "warps_in_flight": opts.warps_in_flight,
                  "lattice": opts.lattice, "weights": "fp32"},
         "autotune": tune,
+        "learned_start": ("half-size grid: n_early iterations + network + 2x upsampling" if coarse is not None
+                          else "n_early iterations + network + priority passes"),
+        "half_grid_setup_s": coarse_setup_s,
         "reference": {"iterations": done + 10 + args.n_early, "cost": ref_cost,
                       "motion_last_10_iterations_hu": ref_motion, "seconds": ref_seconds},
         "plain": brief(plain), "learned": brief(learned),

@@ -1,18 +1,21 @@
 """Train the warm-start network on GPU-generated ICD pairs and evaluate it.
 
-    python -m ctbb_icd_b200.train_warm_start [--train-seeds 100:132] [--heldout-seeds 900:904]
+    python -m ctbb_icd_b200.train_warm_start [--train-seeds 100:300] [--heldout-seeds 900:920]
         [--steps 1500] [--out ctbb_icd_b200/weights/warm_start.npz] [--report report.json]
 
 1. For each seed: synthetic scan of the training geometry (cfg2's scanner,
-   flying focal spot, penalty and 0.6 mm voxels, 512 x 512 x 16), n_early
-   plain grouped-ICD iterations from the zero start (the network's input),
-   then plain ICD to a relative cost change below 1e-7 per iteration (the
+   flying focal spot, phantom and penalty, 256 x 256 over the 30 cm field of
+   view, 32 slices of 0.6 mm; learned.TRAIN_WORKLOAD), n_early plain
+   grouped-ICD iterations from the zero start (the network's input), then
+   plain ICD to a relative cost change below 1e-7 per iteration (the
    target); both rotated to the fixed frame, interior slices kept. Grouped
-   ICD runs with autotuned warps in flight and tile edge.
+   ICD runs with autotuned warps in flight and tile edge. One matrix serves
+   every seed (same geometry).
 2. Adam on random crops (8 x 128 x 128) of the training pairs.
 3. Held-out seeds: loss before and after training, and time to <= 0.5 HU
    RMSE against the plain converged image for plain ICD and for the learned
-   warm start.
+   warm start on the training grid. Full-size (512 x 512 x 64) evaluation:
+   python -m ctbb_icd_b200.eval_warm_start.
 """
 from __future__ import annotations
 
@@ -32,8 +35,8 @@ def _seeds(spec: str):
 
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
-    ap.add_argument("--train-seeds", default="100:132")
-    ap.add_argument("--heldout-seeds", default="900:904")
+    ap.add_argument("--train-seeds", default="100:300")
+    ap.add_argument("--heldout-seeds", default="900:920")
     ap.add_argument("--steps", type=int, default=1500)
     ap.add_argument("--batch", type=int, default=4)
     ap.add_argument("--lr", type=float, default=1e-3)

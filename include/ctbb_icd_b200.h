@@ -342,6 +342,11 @@ ctbb_status ctbb_gpu_recon_set_volume(ctbb_recon* rc, const ctbb_ssm* ssm, const
  * zero projection. ctbb_gpu_icd uses ZERO in sequential (parity) mode unless
  * geom->wfbp_initialize is set, and FORWARD in grouped mode. */
 enum { CTBB_ESTIMATE_ZERO = 0, CTBB_ESTIMATE_FORWARD = 1 };
+/* Multi-resolution start (no reference counterpart): the current image of
+ * `coarse` (same scan, slices and field of view, half the in-plane voxel
+ * count) upsampled 2x in-plane by bilinear interpolation becomes the image of
+ * `fine`, and e = y - A x is recomputed in FP64, device to device. */
+ctbb_status ctbb_gpu_recon_set_volume_upsampled(ctbb_recon* fine, const ctbb_ssm* fine_ssm, ctbb_recon* coarse);
 ctbb_status ctbb_gpu_recon_set_volume_estimate(ctbb_recon* rc, const ctbb_ssm* ssm, const float* vol_host,
                                                int32_t estimate);
 ctbb_status ctbb_gpu_recon_get_volume(ctbb_recon* rc, float* vol_host);

@@ -39,7 +39,10 @@ def test_rmse_hu():
 
 def test_workload_shapes():
     assert L.workload_shape("cfg2") == (64, 512, 512)
-    assert L.workload_shape(L.TRAIN_WORKLOAD) == (16, 512, 512)
+    # the training grid (256 x 256 x 32 over cfg2's field of view) is the
+    # half-size grid of the benchmark scan in-plane
+    assert L.workload_shape(L.TRAIN_WORKLOAD) == (32, 256, 256)
+    assert L.workload_shape(L.coarse_workload("cfg2")) == (64, 256, 256)
 
 
 def test_committed_weights_and_protocol():
