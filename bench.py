@@ -169,11 +169,12 @@ def run_ours(args, rank, world, dist):
         rc.iterate(ssm, 3, opts)
         opts, trials = rc.autotune(ssm, opts, probe_iters=2)
         tune = {"chosen": {"warps_per_voxel": opts.warps_per_voxel, "warps_in_flight": opts.warps_in_flight,
-                           "entries_per_lane": opts.entries_per_lane, "lattice": opts.lattice},
+                           "entries_per_lane": opts.entries_per_lane, "lattice": opts.lattice,
+                           "stage_column": opts.stage_column},
                 "trials": [[t["warps_per_voxel"], t["warps_in_flight"], t["entries_per_lane"], t["lattice"],
-                            round(t["device_ms"], 1), round(t["score"], 1)] for t in trials],
+                            t["stage_column"], round(t["device_ms"], 1), round(t["score"], 1)] for t in trials],
                 "trial_fields": ["warps_per_voxel", "warps_in_flight", "entries_per_lane", "lattice",
-                                 "ms_2_iterations", "cost_decrease_per_ms"]}
+                                 "stage_column", "ms_2_iterations", "cost_decrease_per_ms"]}
         rc.set_volume(ssm, None)
 
     rc.iterate(ssm, args.warmup, opts)
@@ -383,8 +384,9 @@ def _stage_batch(args, C, ctx, torch, clocks):
     GPU through the batched persistent kernel (one launch per iteration for
     all scans of a batch, replayed from a CUDA graph). Scans are packed into
     batches that fit in device memory (a scan that does not fit starts the
-    next batch). For each batch the first three iterations try 0.5, 1 and 2
-    times the default concurrency and the remaining 17 use the fastest.
+    next batch). For each batch the first three iterations try the streamed
+    kernel at 1 and 2 times the default concurrency and the shared-memory
+    staged kernel, and the remaining 17 use the fastest.
     Metric: voxel updates of all scans over the device time of the ICD
     launches; the wall-clock rate including each scan's set-up (projector,
     matrix build, visiting order) is reported beside it."""
@@ -433,25 +435,28 @@ def _stage_batch(args, C, ctx, torch, clocks):
         n_vox = sum(int(np.prod(x[1].shape)) for x in scans)
         base = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32)
         default_w = _batch_default_warps(ctx, [x[1] for x in scans])
-        st0 = b.iterate(1, base)
-        trials = [(default_w, st0.device_ms, st0.entries)]
-        for mult in (0.5, 2.0):
-            w = max(4, int(default_w * mult))
-            st = b.iterate(1, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=w))
-            trials.append((w, st.device_ms, st.entries))
-        best_w = min(trials, key=lambda t: t[1])[0]
-        st = b.iterate(n_iter - 3, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=best_w))
-        dev_ms = sum(t[1] for t in trials) + st.device_ms
+        trials = []
+        # (warps in flight, column stage): the streamed kernel at the default
+        # and twice the default concurrency, the shared-memory staged kernel.
+        for w, stage in ((default_w, 0), (max(4, 2 * default_w), 0), (4 * 148, 1)):
+            st = b.iterate(1, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=w,
+                                         stage_column=stage))
+            trials.append((w, stage, st.device_ms, st.entries))
+        best = min(trials, key=lambda t: t[2])
+        st = b.iterate(n_iter - 3, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP32, warps_in_flight=best[0],
+                                             stage_column=best[1]))
+        dev_ms = sum(t[2] for t in trials) + st.device_ms
         totals["updates"] += n_vox * n_iter
         totals["device_ms"] += dev_ms
-        totals["entries"] += sum(t[2] for t in trials) + st.entries
+        totals["entries"] += sum(t[3] for t in trials) + st.entries
         costs = []
         for _, _, rc, ssm in scans:
             rc.refresh_residual(ssm)
             costs.append(rc.cost())
         batches.append({"scans": [specs[x[0]]["name"] for x in scans], "voxels": n_vox,
-                        "warps_in_flight": best_w, "trials_ms": [[t[0], round(t[1], 2)] for t in trials],
-                        "device_ms": round(dev_ms, 1)})
+                        "warps_in_flight": best[0], "stage_column": best[1],
+                        "trials_ms": [[t[0], t[1], round(t[2], 2)] for t in trials], "device_ms": round(dev_ms, 1),
+                        "fp64_costs_after": costs})
         b.free()
         for _, _, rc, ssm in scans:
             rc.free()

@@ -473,6 +473,75 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
 // e; after the penalty step the scatter reads the entries back from shared
 // memory, latest-gathered first (their e sectors are the likeliest to still
 // be in L2). Columns longer than `cap` re-read their tail from HBM.
+// One voxel update by one warp with the column staged in shared memory
+// (sq / sw: this warp's `cap` stage positions); counts an update that
+// scattered in n_upd / n_ent.
+template <class WT, int U>
+__device__ __forceinline__ void staged_item(const GParams& P, const uint32_t* __restrict__ order,
+                                            const int64_t* __restrict__ colptr, const uint32_t* __restrict__ vptr,
+                                            const int32_t* __restrict__ idx, const WT* __restrict__ w,
+                                            const int32_t* __restrict__ start, float* e, float* x, uint64_t item,
+                                            int lane, int32_t* sq, typename WBits<WT>::T* sw, int cap,
+                                            uint64_t stream, unsigned long long& n_ent, unsigned long long& n_upd) {
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint32_t packed = __ldg(order + item);
+    const uint64_t col = packed / (uint32_t)P.nz;
+    const int k = (int)(packed % (uint32_t)P.nz);
+    const int64_t q = (int64_t)col + (int64_t)ncol * k;
+    const int s = start[k];
+    const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+    int64_t b = 0, en = 0, mid = 0;
+    if (v1 > v0) {
+        const int64_t cb = colptr[col];
+        const uint32_t* vp = vptr + col * P.nvsm1;
+        b = cb + vp[v0];
+        en = cb + vp[v1];
+        // Same common start view for the members of a slice stack as
+        // process_item.
+        const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1),
+                           ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
+        const int vs = min(max(start[kl] - s, v0), v1);
+        mid = cb + vp[vs];
+    }
+    const int off = s * P.nch * P.nr;
+    const int64_t n1 = en - mid, n = en - b;
+
+    float acc_b = 0.f, acc_a = 0.f;
+    stage_gather<WT, U>(idx, w, e, mid, en, 0, off, lane, stream, sq, sw, cap, acc_b, acc_a);
+    stage_gather<WT, U>(idx, w, e, b, mid, n1, off, lane, stream, sq, sw, cap, acc_b, acc_a);
+    const double beta = (double)warp_sum(acc_b);
+    const double alpha = (double)warp_sum(acc_a);
+
+    const double xq = (double)__ldcg(x + q);
+    double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+    if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+    if (lane == 0) x[q] = (float)(xq + upd);
+    const float du = (float)upd;
+    __syncwarp();  // stage writes of every lane visible to the scatter
+    if (du != 0.f) {
+        // Positions [cap, n) were not staged: re-read them (last first).
+        for (int64_t p = n - 1 - lane; p >= cap; p -= 32) {
+            const int64_t m = p < n1 ? mid + p : b + (p - n1);
+            atomicAdd(e + (ld_idx(idx + m, stream) + off), -du * WBits<WT>::value(WBits<WT>::load(w, m, stream)));
+        }
+        const int64_t ns = n < cap ? n : cap;
+        int64_t p = ns - 1 - lane;
+        for (; p >= 32 * 3; p -= 32 * 4) {
+            const int32_t q0 = sq[p], q1 = sq[p - 32], q2 = sq[p - 64], q3 = sq[p - 96];
+            const float w0 = WBits<WT>::value(sw[p]), w1 = WBits<WT>::value(sw[p - 32]);
+            const float w2 = WBits<WT>::value(sw[p - 64]), w3 = WBits<WT>::value(sw[p - 96]);
+            atomicAdd(e + q0, -du * w0);
+            atomicAdd(e + q1, -du * w1);
+            atomicAdd(e + q2, -du * w2);
+            atomicAdd(e + q3, -du * w3);
+        }
+        for (; p >= 0; p -= 32) atomicAdd(e + sq[p], -du * WBits<WT>::value(sw[p]));
+        n_ent += (unsigned long long)n;
+        ++n_upd;
+    }
+    __syncwarp();  // stage reads done before the next item overwrites it
+}
+
 template <class WT, int U, int NW>
 __global__ void __launch_bounds__(32 * NW, 1) icd_staged_kernel(GParams P, const uint32_t* __restrict__ order,
                                                                 const int64_t* __restrict__ colptr,
@@ -487,7 +556,6 @@ __global__ void __launch_bounds__(32 * NW, 1) icd_staged_kernel(GParams P, const
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
     int32_t* sq = reinterpret_cast<int32_t*>(stage_smem) + (size_t)wid * cap;
     SW* sw = reinterpret_cast<SW*>(reinterpret_cast<int32_t*>(stage_smem) + (size_t)NW * cap) + (size_t)wid * cap;
-    const uint64_t ncol = (uint64_t)P.nx * P.ny;
     const uint64_t stream = l2_drop();
     unsigned long long n_ent = 0, n_upd = 0;
     for (;;) {
@@ -495,61 +563,7 @@ __global__ void __launch_bounds__(32 * NW, 1) icd_staged_kernel(GParams P, const
         if (lane == 0) item = atomicAdd(queue, 1ull);
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= P.n_items) break;
-        const uint32_t packed = __ldg(order + item);
-        const uint64_t col = packed / (uint32_t)P.nz;
-        const int k = (int)(packed % (uint32_t)P.nz);
-        const int64_t q = (int64_t)col + (int64_t)ncol * k;
-        const int s = start[k];
-        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
-        int64_t b = 0, en = 0, mid = 0;
-        if (v1 > v0) {
-            const int64_t cb = colptr[col];
-            const uint32_t* vp = vptr + col * P.nvsm1;
-            b = cb + vp[v0];
-            en = cb + vp[v1];
-            // Same common start view for the members of a slice stack as
-            // process_item.
-            const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1), ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
-            const int vs = min(max(start[kl] - s, v0), v1);
-            mid = cb + vp[vs];
-        }
-        const int off = s * P.nch * P.nr;
-        const int64_t n1 = en - mid, n = en - b;
-
-        float acc_b = 0.f, acc_a = 0.f;
-        stage_gather<WT, U>(idx, w, e, mid, en, 0, off, lane, stream, sq, sw, cap, acc_b, acc_a);
-        stage_gather<WT, U>(idx, w, e, b, mid, n1, off, lane, stream, sq, sw, cap, acc_b, acc_a);
-        const double beta = (double)warp_sum(acc_b);
-        const double alpha = (double)warp_sum(acc_a);
-
-        const double xq = (double)__ldcg(x + q);
-        double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
-        if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
-        if (lane == 0) x[q] = (float)(xq + upd);
-        const float du = (float)upd;
-        __syncwarp();  // stage writes of every lane visible to the scatter
-        if (du != 0.f) {
-            // Positions [cap, n) were not staged: re-read them (last first).
-            for (int64_t p = n - 1 - lane; p >= cap; p -= 32) {
-                const int64_t m = p < n1 ? mid + p : b + (p - n1);
-                atomicAdd(e + (ld_idx(idx + m, stream) + off), -du * WBits<WT>::value(WBits<WT>::load(w, m, stream)));
-            }
-            const int64_t ns = n < cap ? n : cap;
-            int64_t p = ns - 1 - lane;
-            for (; p >= 32 * 3; p -= 32 * 4) {
-                const int32_t q0 = sq[p], q1 = sq[p - 32], q2 = sq[p - 64], q3 = sq[p - 96];
-                const float w0 = WBits<WT>::value(sw[p]), w1 = WBits<WT>::value(sw[p - 32]);
-                const float w2 = WBits<WT>::value(sw[p - 64]), w3 = WBits<WT>::value(sw[p - 96]);
-                atomicAdd(e + q0, -du * w0);
-                atomicAdd(e + q1, -du * w1);
-                atomicAdd(e + q2, -du * w2);
-                atomicAdd(e + q3, -du * w3);
-            }
-            for (; p >= 0; p -= 32) atomicAdd(e + sq[p], -du * WBits<WT>::value(sw[p]));
-            n_ent += (unsigned long long)n;
-            ++n_upd;
-        }
-        __syncwarp();  // stage reads done before the next item overwrites it
+        staged_item<WT, U>(P, order, colptr, vptr, idx, w, start, e, x, item, lane, sq, sw, cap, stream, n_ent, n_upd);
     }
     flush_counts(stats, n_upd, n_ent, lane);
 }
@@ -690,6 +704,34 @@ __global__ void __launch_bounds__(256) icd_batch_kernel(const ScanRefs<WT>* __re
         GParams P = S.P;
         P.relax = relax;
         process_item(P, S.order, S.colptr, S.vptr, S.idx, S.w, S.start, S.e, S.x, m & ((1ull << 40) - 1), lane);
+    }
+}
+
+// Batched variant of icd_staged_kernel (the column of each update staged in
+// shared memory, 4 updates per CTA).
+template <class WT>
+__global__ void __launch_bounds__(128, 1) icd_batch_staged_kernel(const ScanRefs<WT>* __restrict__ scans,
+                                                                  const uint64_t* __restrict__ merged,
+                                                                  uint64_t n_total, double relax,
+                                                                  unsigned long long* queue, int cap) {
+    using SW = typename WBits<WT>::T;
+    extern __shared__ __align__(16) unsigned char stage_smem[];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int32_t* sq = reinterpret_cast<int32_t*>(stage_smem) + (size_t)wid * cap;
+    SW* sw = reinterpret_cast<SW*>(reinterpret_cast<int32_t*>(stage_smem) + (size_t)4 * cap) + (size_t)wid * cap;
+    const uint64_t stream = l2_drop();
+    unsigned long long n_ent = 0, n_upd = 0;
+    for (;;) {
+        unsigned long long t = 0;
+        if (lane == 0) t = atomicAdd(queue, 1ull);
+        t = __shfl_sync(0xffffffffu, t, 0);
+        if (t >= n_total) break;
+        const uint64_t m = __ldg(merged + t);
+        const ScanRefs<WT>& S = scans[m >> 40];
+        GParams P = S.P;
+        P.relax = relax;
+        staged_item<WT, 16>(P, S.order, S.colptr, S.vptr, S.idx, S.w, S.start, S.e, S.x, m & ((1ull << 40) - 1), lane,
+                            sq, sw, cap, stream, n_ent, n_upd);
     }
 }
 
@@ -1234,7 +1276,7 @@ struct ctbb_batch {
     std::vector<int> merged_T;  // tile edge per scan when d_merged was built
     void* d_scans = nullptr;
     cudaGraphExec_t graph = nullptr;
-    int graph_warps = 0, graph_weights = 0;
+    int graph_warps = 0, graph_weights = 0, graph_stage = 0;
     double graph_relax = 0.0;
 };
 
@@ -1312,15 +1354,27 @@ void drop_graph(ctbb_batch* b) {
 }
 
 template <class WT>
-ctbb_status capture_iteration(ctbb_batch* b, int warps, double relax) {
+ctbb_status capture_iteration(ctbb_batch* b, int warps, double relax, int stage) {
     drop_graph(b);
     cudaStream_t st = b->ctx->stream;
-    const int blocks = std::max(1, (warps + 7) / 8);
+    const int cap = stage_capacity(b->ctx, 4, (int)sizeof(WT));
+    const size_t smem = (size_t)4 * cap * (4 + sizeof(WT));
+    if (stage)
+        CTBB_CUDA(cudaFuncSetAttribute(icd_batch_staged_kernel<WT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)smem));
     cudaGraph_t g = nullptr;
     CTBB_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     cudaMemsetAsync(b->ctx->d_queue, 0, sizeof(unsigned long long), st);
-    icd_batch_kernel<WT><<<blocks, 256, 0, st>>>((const ScanRefs<WT>*)b->d_scans, b->d_merged, b->n_total, relax,
-                                                 b->ctx->d_queue);
+    if (stage) {
+        // One CTA of 4 staged updates per SM.
+        const int blocks = std::max(1, std::min(b->ctx->sm_count, (warps + 3) / 4));
+        icd_batch_staged_kernel<WT><<<blocks, 128, smem, st>>>((const ScanRefs<WT>*)b->d_scans, b->d_merged,
+                                                               b->n_total, relax, b->ctx->d_queue, cap);
+    } else {
+        const int blocks = std::max(1, (warps + 7) / 8);
+        icd_batch_kernel<WT><<<blocks, 256, 0, st>>>((const ScanRefs<WT>*)b->d_scans, b->d_merged, b->n_total,
+                                                     relax, b->ctx->d_queue);
+    }
     const cudaError_t le = cudaGetLastError();
     const cudaError_t ce = cudaStreamEndCapture(st, &g);
     if (le != cudaSuccess || ce != cudaSuccess) {
@@ -1417,14 +1471,18 @@ extern "C" ctbb_status ctbb_gpu_batch_iterate(ctbb_batch* b, const ctbb_icd_opts
                            (double)b->n_total / (double)rc->n_order;
         warps = std::max(1, std::min(warps, (int)cap));
     }
-    if (!b->graph || b->graph_warps != warps || b->graph_relax != relax || b->graph_weights != wsel) {
+    const int stage = o.stage_column ? 1 : 0;
+    if (stage) warps = std::min(warps, b->ctx->sm_count * 4);
+    if (!b->graph || b->graph_warps != warps || b->graph_relax != relax || b->graph_weights != wsel ||
+        b->graph_stage != stage) {
         if (wsel == CTBB_SSM_FP16) {
             CTBB_TRY(upload_scans<__half>(b, o));
-            CTBB_TRY(capture_iteration<__half>(b, warps, relax));
+            CTBB_TRY(capture_iteration<__half>(b, warps, relax, stage));
         } else {
             CTBB_TRY(upload_scans<float>(b, o));
-            CTBB_TRY(capture_iteration<float>(b, warps, relax));
+            CTBB_TRY(capture_iteration<float>(b, warps, relax, stage));
         }
+        b->graph_stage = stage;
         b->graph_warps = warps;
         b->graph_relax = relax;
         b->graph_weights = wsel;
