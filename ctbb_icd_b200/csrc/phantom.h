@@ -174,6 +174,12 @@ struct ctbb_ray_geom {
     double tube_angle_increment, z_first_view, tube_z_increment;
     int32_t table_direction, phi_ffs;
     int64_t n_channels, n_rows, readings;
+    // z flying focal spot (generate_system_matrix_ffs.cpp:66, :266-285): the
+    // source moves by -/+dr along e_w and -/+dz along z (dz = dr * tan of the
+    // anode angle taken in radians, as the reference evaluates it); with both
+    // spots the in-plane offset cycles over four views.
+    int32_t z_ffs, any_ffs;
+    double dr, dz;
 };
 
 // Unit ray (start s, direction u) of data view g, channel j, row r.
@@ -182,7 +188,7 @@ CTBB_HD void ctbb_ray(const ctbb_ray_geom& G, int64_t g, int64_t j, int64_t r, d
     const double th = (double)g * G.tube_angle_increment;
     const double ct = cos(th), st = sin(th);
     const double zg = G.z_first_view + (double)g * (double)G.table_direction * G.tube_z_increment;
-    const double gam = G.phi_ffs ? ((double)j - G.cc) * G.fan_inc : ((double)j - G.cc) * G.s_t / G.SDD;
+    const double gam = G.any_ffs ? ((double)j - G.cc) * G.fan_inc : ((double)j - G.cc) * G.s_t / G.SDD;
     const double cg = cos(gam), sg = sin(gam);
     const double ax = ((double)r - G.cr) * G.s_a;
     double off = 0.0;
@@ -192,9 +198,26 @@ CTBB_HD void ctbb_ray(const ctbb_ray_geom& G, int64_t g, int64_t j, int64_t r, d
     const double b0 = S0 - G.SDD * cg * ct + G.SDD * sg * st;
     const double b1 = S1 - G.SDD * cg * st - G.SDD * sg * ct;
     const double b2 = S2 - ax;
-    s[0] = S0 - off * st;
-    s[1] = S1 + off * ct;
-    s[2] = S2;
+    if (G.z_ffs) {
+        // generate_system_matrix_ffs.cpp:266-285
+        double sr, sa;
+        if (G.phi_ffs) {
+            const int64_t rho = g % 4;
+            sr = rho < 2 ? -1.0 : 1.0;
+            sa = (rho % 2 == 0) ? -1.0 : 1.0;
+        } else {
+            sr = (g % 2 == 0) ? -1.0 : 1.0;
+            sa = 0.0;
+        }
+        const double ow = sr * G.dr, ou = sa * G.da, oz = sr * G.dz;
+        s[0] = S0 + ow * ct - ou * st;
+        s[1] = S1 + ow * st + ou * ct;
+        s[2] = S2 + oz;
+    } else {
+        s[0] = S0 - off * st;
+        s[1] = S1 + off * ct;
+        s[2] = S2;
+    }
     double d0 = b0 - s[0], d1 = b1 - s[1], d2 = b2 - s[2];
     const double n = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
     u[0] = d0 / n;
@@ -270,7 +293,14 @@ inline ctbb_ray_geom ctbb_ray_geom_from(const G& g) {
     r.z_first_view = g.z_first_view;
     r.tube_z_increment = g.tube_z_increment;
     r.table_direction = (int32_t)g.table_direction;
-    r.phi_ffs = (g.Phiffs != 0 && g.Zffs == 0) ? 1 : 0;
+    r.phi_ffs = g.Phiffs != 0 ? 1 : 0;
+    r.z_ffs = g.Zffs != 0 ? 1 : 0;
+    r.any_ffs = (g.Phiffs != 0 || g.Zffs != 0) ? 1 : 0;
+    // generate_system_matrix_ffs.cpp:66 (its PI is 3.14159265359) and the
+    // tan(anode_angle) of :272 with the angle in degrees.
+    r.dr = g.source_detector_distance * g.CollSlicewidth /
+           (4.0 * (g.source_detector_distance - g.focal_spot_radius) * tan(g.anode_angle * 3.14159265359 / 180.0));
+    r.dz = r.dr * tan(g.anode_angle);
     r.n_channels = (int64_t)g.n_channels;
     r.n_rows = (int64_t)g.Nrows_projection;
     r.readings = (int64_t)g.Readings;

@@ -123,8 +123,10 @@ __device__ __forceinline__ void row_range(const SsmParams& P, const ViewTab& V, 
         *r_hi = P.nr - 1;
         return;
     }
+    // z(k) = src2 - ((k - cr) sa + off2) L: the z deflection of a z flying
+    // focal spot shifts the rows by -off2 / sa.
     double a = V.src2 - P.vz, b = V.src2 + P.vz;  // k_hat in [-1, 1)  <=>  z in [-vz, vz)
-    double k0 = P.cr + a / (P.sa * L), k1 = P.cr + b / (P.sa * L);
+    double k0 = P.cr + a / (P.sa * L) - V.off2 / P.sa, k1 = P.cr + b / (P.sa * L) - V.off2 / P.sa;
     if (k0 > k1) {
         const double t = k0;
         k0 = k1;
@@ -150,14 +152,15 @@ __global__ void __launch_bounds__(256) ssm_cells_kernel(
         const ViewTab V = vt[v];
         // Candidate channels: rays through the two sampling segments of this
         // column (vertical at x_ic for x-major rays, horizontal at y_jc for
-        // y-major rays), padded by one channel for rounding and by two with
-        // the flying focal spot (the deflected source shifts a ray by < 0.5
-        // channel relative to the nominal fan model used for the bound).
+        // y-major rays), padded by one channel for rounding and by three with
+        // a flying focal spot (the deflected source shifts a ray by about a
+        // channel at the fan edge relative to the nominal fan model used for
+        // the bound).
         const double xc = (ic - P.cvx) * P.vx, yc = (jc - P.cvy) * P.vy;
         const double c0 = chan_of(P, V, xc, yc - P.vy), c1 = chan_of(P, V, xc, yc + P.vy);
         const double c2 = chan_of(P, V, xc - P.vx, yc), c3 = chan_of(P, V, xc + P.vx, yc);
         const double cmin = fmin(fmin(c0, c1), fmin(c2, c3)), cmax = fmax(fmax(c0, c1), fmax(c2, c3));
-        const int pad = P.ffs ? 2 : 1;
+        const int pad = P.ffs ? 3 : 1;
         const int ch_lo = max((int)floor(cmin) - pad, 0);
         const int ch_hi = min((int)ceil(cmax) + pad, P.nch - 1);
         uint32_t n = 0;
@@ -289,6 +292,8 @@ void host_tables(const ctbb_geom_c& g, std::vector<ViewTab>& vt, std::vector<dou
     const size_t nvsm = g.num_views_for_system_matrix;
     const double SDD = g.source_detector_distance, R = g.focal_spot_radius;
     const double da = SDD * R * sin(g.fan_angle_increment) / (4.0 * (SDD - R));  // generate_system_matrix_ffs.cpp:67
+    // generate_system_matrix_ffs.cpp:66, with that file's PI (3.14159265359)
+    const double dr = SDD * g.CollSlicewidth / (4.0 * (SDD - R) * tan(g.anode_angle * 3.14159265359 / 180.0));
     vt.resize(nvsm);
     for (int i = 0; i < (int)nvsm; ++i) {
         const double ta = (i - 0.5 * nvsm) * g.tube_angle_increment;  // generate_system_matrix.cpp:85
@@ -302,11 +307,29 @@ void host_tables(const ctbb_geom_c& g, std::vector<ViewTab>& vt, std::vector<dou
         V.src1 = R * V.ew1 + zs * 0.0;
         V.src2 = R * 0.0 + zs * 1.0;
         V.off0 = V.off1 = V.off2 = 0.0;
-        if (ffs) {
+        if (ffs && !g.Zffs) {
             const double s = (i % 2 == 0) ? da : -da;  // generate_system_matrix_ffs.cpp:253-259
             V.off0 = s * V.eu0;
             V.off1 = s * V.eu1;
             V.off2 = s * 0.0;
+        } else if (ffs && !g.Phiffs) {
+            // generate_system_matrix_ffs.cpp:262-270: -/+dr e_w -/+dr tan(anode_angle) e_z
+            // (the anode angle passed in degrees to tan, as the reference does)
+            const double r = (i % 2 == 0) ? -dr : dr;
+            const double t = tan(g.anode_angle);
+            V.off0 = r * V.ew0 + (r * t) * 0.0;
+            V.off1 = r * V.ew1 + (r * t) * 0.0;
+            V.off2 = r * 0.0 + (r * t) * 1.0;
+        } else if (ffs) {
+            // generate_system_matrix_ffs.cpp:272-284: four deflections per cycle
+            const int rho = i % 4;
+            const double r = rho < 2 ? -dr : dr, a = (rho % 2 == 0) ? -da : da;
+            const double t = tan(g.anode_angle);
+            V.off0 = (r * V.ew0 + a * V.eu0) + (r * t) * 0.0;
+            V.off1 = (r * V.ew1 + a * V.eu1) + (r * t) * 0.0;
+            V.off2 = (r * 0.0 + a * 0.0) + (r * t) * 1.0;
+        }
+        if (ffs) {
             V.src0 = V.src0 + V.off0;  // generate_system_matrix_ffs.cpp:134
             V.src1 = V.src1 + V.off1;
             V.src2 = V.src2 + V.off2;
@@ -361,7 +384,7 @@ ctbb_status ssm_validate_geometry(const ctbb_geom_c& g) {
         return fail(CTBB_ERR_INVALID_ARG, "need at least 2x2 voxels per slice");
     if (g.n_channels == 0 || g.Nrows_projection == 0 || g.num_views_for_system_matrix == 0)
         return fail(CTBB_ERR_INVALID_ARG, "empty detector or system-matrix window");
-    if (g.Zffs != 0) return fail(CTBB_ERR_UNSUPPORTED, "z flying focal spot is not supported");
+    if (g.Zffs > 1 || g.Phiffs > 1) return fail(CTBB_ERR_INVALID_ARG, "Zffs and Phiffs are 0 or 1");
     const double q = (double)g.num_views_for_system_matrix * g.n_channels * g.Nrows_projection;
     const double ds = (double)g.Readings * g.n_channels * g.Nrows_projection;
     if (q >= 2147483647.0 || ds >= 2147483647.0)

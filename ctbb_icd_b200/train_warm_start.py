@@ -47,6 +47,8 @@ def main(argv=None):
     ap.add_argument("--prio-passes", type=int, default=2)
     ap.add_argument("--eval-scans", type=int, default=2)
     ap.add_argument("--pairs", default=None, help="npz cache of the generated pairs (read if present, else written)")
+    ap.add_argument("--engine", choices=["tcgen05", "mma_sync"], default="tcgen05",
+                    help="tensor-core path of the 32 -> 32 convolutions")
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)
     args = ap.parse_args(argv)
@@ -67,6 +69,7 @@ def main(argv=None):
     # The early-iterate protocol the network is trained for (and recorded
     # with its weights): the tuned tile edge and density of in-flight updates.
     net = L.WarmStartNet(ctx, args.blocks, seed=0)
+    net.set_engine(C.CNN_ENGINE_TCGEN05 if args.engine == "tcgen05" else C.CNN_ENGINE_MMA_SYNC)
     nvox = int(np.prod(L.workload_shape(L.TRAIN_WORKLOAD)))
     net.n_early = args.n_early
     net.early_lattice = int(opts.lattice)

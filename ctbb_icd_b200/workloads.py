@@ -19,7 +19,7 @@ widths are quoted at isocentre and converted to the detector
         5e4..2e5, 512 x 512 x 64 at 0.6 mm, 30 cm FOV, edge-preserving with
         delta = 5 HU (9.6e-4 cm^-1) and lambda = 0.1 (the value of the
         reference's resources/sample_prm.yaml; the benchmark names none).
-  tiny, tiny_ffs, small, small_ffs, mid
+  tiny, tiny_ffs, tiny_zffs, tiny_zphiffs, small, small_ffs, mid
         reduced geometries (few channels/rows/views, large voxels) that the
         reference program finishes in seconds: golden fixtures and parity
         tests.
@@ -142,6 +142,23 @@ WORKLOADS = {
              **_scanner(48, 23.75, 0.00882, 4, 1.5, 128, True, 1.0, 5),
              **_recon(12, 25.0, 1.5, 3, -5.0, "edge-preserving", 0.5, 0.005, 3)},
         phantom=dict(n_ellipsoids=3, seed=2, i0_lo=5e4, i0_hi=2e5, z_lo=-9.0, z_hi=-5.0),
+    ),
+    # tiny_ffs with the z flying focal spot (z only, and z + in-plane): each
+    # projection has Nrows / 2 = 2 rows (setup.cpp:225) and the views per
+    # turn double (quadruple with both spots).
+    "tiny_zffs": dict(
+        prm={**_BASE,
+             **_scanner(48, 23.75, 0.00882, 4, 1.5, 128, True, 1.0, 5),
+             "Zffs": 1, "Phiffs": 0, "center_row": 0.5,
+             **_recon(12, 25.0, 1.5, 3, -5.0, "edge-preserving", 0.5, 0.005, 3)},
+        phantom=dict(n_ellipsoids=3, seed=6, i0_lo=5e4, i0_hi=2e5, z_lo=-9.0, z_hi=-5.0),
+    ),
+    "tiny_zphiffs": dict(
+        prm={**_BASE,
+             **_scanner(48, 23.75, 0.00882, 4, 1.5, 128, True, 1.0, 5),
+             "Zffs": 1, "Phiffs": 1, "center_row": 0.5, "Readings": 5 * 512,
+             **_recon(12, 25.0, 1.5, 3, -5.0, "quadratic", 0.5, 0.005, 3)},
+        phantom=dict(n_ellipsoids=3, seed=7, i0_lo=5e4, i0_hi=2e5, z_lo=-9.0, z_hi=-5.0),
     ),
     "small": dict(
         prm={**_BASE,

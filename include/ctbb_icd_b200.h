@@ -228,14 +228,18 @@ typedef struct ctbb_ssm_info {
     uint64_t max_col_nnz;   /* largest column                              */
     uint64_t bytes_device;  /* device bytes held by the matrix             */
     int32_t weights;        /* CTBB_SSM_* held                             */
-    int32_t ffs;            /* 1 if built with the in-plane flying focal spot */
+    int32_t ffs;            /* 1 if built with a flying focal spot (in-plane and/or z) */
     double build_ms;        /* device time of the last build               */
 } ctbb_ssm_info;
 
 /*
  * Build the stored system matrix on the device: per voxel column (i + nx*j),
  * entries (q, w) with q = row + Nrows*(channel + n_channels*view), sorted by q.
- * Chooses the in-plane FFS model when geom->Phiffs is set.
+ * Chooses the flying-focal-spot model from geom->Phiffs / geom->Zffs like
+ * main.cpp:103-109: in-plane (Phi), z (Z) or both, with the source offsets of
+ * generate_ffs_offset (generate_system_matrix_ffs.cpp:242-290) as the
+ * reference evaluates them (including its z deflection dr * tan(anode_angle)
+ * with the angle in degrees passed to tan).
  * Replaces generate_system_matrix (src/generate_system_matrix.cpp:54-209) and
  * generate_system_matrix_ffs (src/generate_system_matrix_ffs.cpp:60-239);
  * the on-disk matrix.bin round trip (:212-303) becomes an HBM-resident matrix.

@@ -147,6 +147,12 @@ struct ViewGeom {
     double src0, src1, src2, off0, off1, off2;
 };
 
+// generate_system_matrix_ffs.cpp:66 (PI there is 3.14159265359)
+double ffs_dr(const ctbb_geom_c* g) {
+    const double SDD = g->source_detector_distance, R = g->focal_spot_radius;
+    return SDD * g->CollSlicewidth / (4.0 * (SDD - R) * tan(g->anode_angle * 3.14159265359 / 180.0));
+}
+
 ViewGeom view_geom(const ctbb_geom_c* g, int i, bool ffs, double da) {
     ViewGeom v;
     const double nvsm = (double)g->num_views_for_system_matrix;
@@ -159,11 +165,32 @@ ViewGeom view_geom(const ctbb_geom_c* g, int i, bool ffs, double da) {
     v.src1 = g->focal_spot_radius * v.ew1 + zs * v.ez1;
     v.src2 = g->focal_spot_radius * v.ew2 + zs * v.ez2;
     v.off0 = v.off1 = v.off2 = 0.0;
-    if (ffs) {
+    if (ffs && !g->Zffs) {
+        // generate_ffs_offset, Phi only (:253-259): +da e_u on even views.
         const double sdx = (i % 2 == 0) ? da : -da;
         v.off0 = sdx * v.eu0;
         v.off1 = sdx * v.eu1;
         v.off2 = sdx * v.eu2;
+    } else if (ffs && !g->Phiffs) {
+        // Z only (:262-270): -dr e_w - dr tan(anode_angle) e_z on even views,
+        // + on odd; tan of the angle as given (degrees).
+        const double dr = ffs_dr(g);
+        const double c = (i % 2 == 0) ? -dr : dr;
+        const double ct = c * tan(g->anode_angle);
+        v.off0 = c * v.ew0 + ct * v.ez0;
+        v.off1 = c * v.ew1 + ct * v.ez1;
+        v.off2 = c * v.ew2 + ct * v.ez2;
+    } else if (ffs) {
+        // Z and Phi (:272-284): (-dr, -da), (-dr, +da), (+dr, -da), (+dr, +da).
+        const double dr = ffs_dr(g);
+        const int rho = i % 4;
+        const double c = rho < 2 ? -dr : dr, a = (rho % 2 == 0) ? -da : da;
+        const double ct = c * tan(g->anode_angle);
+        v.off0 = (c * v.ew0 + a * v.eu0) + ct * v.ez0;
+        v.off1 = (c * v.ew1 + a * v.eu1) + ct * v.ez1;
+        v.off2 = (c * v.ew2 + a * v.eu2) + ct * v.ez2;
+    }
+    if (ffs) {
         v.src0 = v.src0 + v.off0;
         v.src1 = v.src1 + v.off1;
         v.src2 = v.src2 + v.off2;

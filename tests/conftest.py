@@ -57,7 +57,7 @@ class Golden:
         return Csr(self.colptr, self.idx, self.w)
 
 
-@pytest.fixture(scope="session", params=["tiny", "tiny_ffs"])
+@pytest.fixture(scope="session", params=["tiny", "tiny_ffs", "tiny_zffs", "tiny_zphiffs"])
 def golden(request, tmp_path_factory):
     return Golden(request.param, tmp_path_factory.mktemp(request.param))
 

@@ -85,7 +85,7 @@ def test_port_forward_is_linear(golden):
 def test_port_ssm_subset_equals_full_build_restricted(tmp_path):
     """The column/view-restricted builder (used to check the full-size matrix
     on sampled columns) gives exactly the full builder's entries."""
-    for name in ("tiny", "tiny_ffs", "small_ffs"):
+    for name in ("tiny", "tiny_ffs", "small_ffs", "tiny_zphiffs"):
         _, rp = W.materialise(name, str(tmp_path / name), raw=False)
         full = O.port_ssm(rp)
         ncol = int(rp.geom.nx * rp.geom.ny)
