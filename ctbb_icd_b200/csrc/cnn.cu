@@ -563,7 +563,7 @@ struct ctbb_cnn {
     bool weights_dirty = true;
     // C -> C convolutions: CTBB_CNN_ENGINE_TCGEN05 (cnn_tc.cu) or
     // CTBB_CNN_ENGINE_MMA_SYNC (conv_mid_kernel below).
-    int engine = CTBB_CNN_ENGINE_TCGEN05;
+    int engine = CTBB_CNN_ENGINE_MMA_SYNC;
     // Activation workspace, grown on demand: a_0..a_B, h_0..h_{B-1}, two
     // gradient buffers and du.
     uint64_t cap = 0;
@@ -642,6 +642,7 @@ ctbb_status check_conv_flag(ctbb_cnn* c) {
     CTBB_CUDA(cudaMemcpy(&h, c->ctx->d_flags + 1, sizeof(int), cudaMemcpyDeviceToHost));
     if (h) {
         CTBB_CUDA(cudaMemset(c->ctx->d_flags + 1, 0, sizeof(int)));
+        if (h == 2) return fail(CTBB_ERR_CUDA, "tensor-core convolution: shared memory not aligned for its copies");
         return fail(CTBB_ERR_TIMEOUT, "tensor-core convolution: a wait for its loads or products expired");
     }
     return CTBB_OK;

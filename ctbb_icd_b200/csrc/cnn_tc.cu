@@ -9,7 +9,8 @@
 // 8 channels, row r of a region at byte 16 r):
 //   weights  27 taps x 4 channel chunks x 32 rows (co)          54 KB, once
 //   halo x2  9 input lines (dz, dy in -1..1) x 4 chunks x 130 rows
-//            (x0-1 .. x0+128), one TMA box per (line, chunk)    73 KB each
+//            (x0-1 .. x0+128), one TMA box per (line, chunk), each chunk
+//            region padded to 2176 bytes (128-byte aligned)      77 KB each
 // Tap (dx, dy, dz) reads line (dz, dy) starting at row 1 + dx, so the 27 A
 // operands are descriptors into the same halo (start address shifted by
 // 16 bytes per voxel); the borders come from the TMA's zero fill.
@@ -37,7 +38,10 @@ constexpr int kC = 32;
 constexpr int kTaps = 27;
 constexpr int kM = 128;                         // output voxels per tile
 constexpr int kLine = kM + 2;                   // input voxels per halo line
-constexpr int kChunkBytes = kLine * 16;         // 2080: one 8-channel chunk of a line
+// One 8-channel chunk of a line: kLine rows of 16 bytes (2080), padded to a
+// multiple of 128 bytes because a tiled TMA copy must land on a 128-byte
+// aligned shared-memory address.
+constexpr int kChunkBytes = ((kLine * 16 + 127) / 128) * 128;  // 2176
 constexpr int kLineBytes = 4 * kChunkBytes;     // 8320
 constexpr int kHaloBytes = 9 * kLineBytes;      // 74880
 constexpr int kTapWBytes = 4 * kC * 16;         // 2048
@@ -49,6 +53,9 @@ constexpr int kOffTmem = kOffBar + 4 * 8;
 constexpr int kSmemBytes = kOffTmem + 16;
 constexpr int kThreads = 128;
 constexpr int kTmemCols = 64;                    // two 32-column accumulators
+static_assert(kChunkBytes % 128 == 0 && kLineBytes % 128 == 0 && kHaloBytes % 128 == 0 && kWBytes % 128 == 0,
+              "TMA destinations must stay 128-byte aligned");
+static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16,
 // both K-major, N = 32, M = 128.
@@ -198,6 +205,17 @@ __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_c
     __syncthreads();
     fence_after();
     const uint32_t tmem = *s_tmem;
+    // Every TMA destination is the halo base plus a multiple of 128 bytes:
+    // refuse to issue any copy if the base itself is not 128-byte aligned.
+    if (((s_base + kOffHalo0) & 127u) != 0u) {
+        if (tid == 0) atomicExch(err, 2);
+        fence_before();
+        __syncthreads();
+        fence_after();
+        if (warp == 0)
+            asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+        return;
+    }
 
     // Phase parity of each barrier (bit b), advanced only after a completed wait.
     uint32_t ph_load = 0, ph_mma = 0;
@@ -315,7 +333,8 @@ namespace ctbb {
 
 // C -> C convolution of channels-last BF16 activations `in` [nz][ny][nx][32]
 // with the kernel `wt` [27][co][ci] on the tcgen05 tensor cores; epilogue as
-// conv_mid_kernel. `err` (device) receives 1 if a wait ran out.
+// conv_mid_kernel. `err` (device) receives 1 if a wait ran out, 2 if shared
+// memory was not aligned for the TMA copies (nothing is computed then).
 ctbb_status conv_mid_tc(ctbb_ctx* ctx, int nx, int ny, int nz, const __nv_bfloat16* in, const __nv_bfloat16* wt,
                         const float* bias, const __nv_bfloat16* residual, const __nv_bfloat16* mask, int relu,
                         __nv_bfloat16* out, int* err) {

@@ -2,9 +2,10 @@
 //
 // Replaces rotate_slices_rotating2fixed (rotate_slices.cpp:81-114),
 // rotate_slices_fixed2rotating (:48-79), rotate_slice (:116-154) and interp2
-// (interp.h:41-76). One thread per output pixel gathers its four bilinear
-// taps (an L2-resident slice of at most 1 MB at 512 x 512); the kernel is a
-// pure streaming gather, bounded by HBM bandwidth.
+// (interp.h:41-76). Each thread gathers the four bilinear taps of four
+// output pixels of one row (an L2-resident slice of at most 1 MB at
+// 512 x 512), all loads issued before any is used; the kernel is a
+// streaming gather, bounded by HBM bandwidth.
 //
 // Compiled with -fmad=false. The per-slice cos/sin are computed on the host
 // with the reference's expressions, the rotated coordinates in double and
@@ -21,39 +22,71 @@
 
 namespace {
 
-__global__ void __launch_bounds__(256) rotate_kernel(const float* __restrict__ in, float* __restrict__ out, int nx,
-                                                     int ny, int nz, int dim1, int dim2, int out_stride_y,
-                                                     const double* __restrict__ cs, double cvx, double cvy) {
+// Output pixels per thread (spaced kRotBlock apart along x).
+constexpr int kRotBlock = 128, kRotPix = 4;
+
+// Grid: x = groups of kRotBlock * kRotPix pixels of a row, y = row, z = slice.
+// Each thread issues the 16 bilinear loads of its 4 pixels before using any.
+__global__ void __launch_bounds__(kRotBlock) rotate_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                           int nx, int ny, int nz, int dim1, int dim2,
+                                                           int out_stride_y, const double* __restrict__ cs,
+                                                           double cvx, double cvy) {
+    const int k = blockIdx.z, y_idx = blockIdx.y;
     const uint64_t npix = (uint64_t)nx * ny;
-    const uint64_t n = npix * nz;
-    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < n; t += (uint64_t)gridDim.x * blockDim.x) {
-        const int k = (int)(t / npix);
-        const uint64_t p = t % npix;
-        const int x_idx = (int)(p % nx), y_idx = (int)(p / nx);
-        const double c = cs[2 * k], s = cs[2 * k + 1];
-        const double x = x_idx - cvx, y = y_idx - cvy;
+    const double c = cs[2 * k], s = cs[2 * k + 1];
+    const float* a = in + (uint64_t)k * npix;
+    const double y = y_idx - cvy;
+    float tap[kRotPix][4], vv[kRotPix], ww[kRotPix];
+    bool inside[kRotPix];
+#pragma unroll
+    for (int u = 0; u < kRotPix; ++u) {
+        const int x_idx = blockIdx.x * (kRotBlock * kRotPix) + u * kRotBlock + threadIdx.x;
+        const double x = x_idx - cvx;
         const float xp = (float)(c * x - s * y);
         const float yp = (float)(s * x + c * y);
         const float i1 = (float)((double)xp + cvx);
         const float i2 = (float)((double)yp + cvy);
-        const float* a = in + (uint64_t)k * npix;
-        float val;
-        if (i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0)) {
-            val = 0.0f;
-        } else {
-            const float v = i1 - floorf(i1);
-            const float w = i2 - floorf(i2);
+        // interp.h:57-58: zero outside [0, n-2] in either index.
+        inside[u] = x_idx < nx && !(i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0));
+        vv[u] = i1 - floorf(i1);
+        ww[u] = i2 - floorf(i2);
+        if (inside[u]) {
             const int f1 = (int)floorf(i1), f2 = (int)floorf(i2);
-            const int a1 = f2 * dim1 + f1;
-            const int a2 = f2 * dim1 + f1 + 1;
-            const int a3 = (f2 + 1) * dim1 + f1;
-            const int a4 = (f2 + 1) * dim1 + f1 + 1;
-            val = a[a1] * (1.0f - v) * (1.0f - w) + a[a2] * v * (1.0f - w) + a[a3] * (1.0f - v) * w +
-                  a[a4] * v * w;
+            tap[u][0] = __ldg(a + (f2 * dim1 + f1));
+            tap[u][1] = __ldg(a + (f2 * dim1 + f1 + 1));
+            tap[u][2] = __ldg(a + ((f2 + 1) * dim1 + f1));
+            tap[u][3] = __ldg(a + ((f2 + 1) * dim1 + f1 + 1));
         }
+    }
+#pragma unroll
+    for (int u = 0; u < kRotPix; ++u) {
+        const int x_idx = blockIdx.x * (kRotBlock * kRotPix) + u * kRotBlock + threadIdx.x;
+        if (x_idx >= nx) continue;
+        const float v = vv[u], w = ww[u];
+        // interp.h:70-73, the reference's operation order.
+        const float val = inside[u] ? tap[u][0] * (1.0f - v) * (1.0f - w) + tap[u][1] * v * (1.0f - w) +
+                                          tap[u][2] * (1.0f - v) * w + tap[u][3] * v * w
+                                    : 0.0f;
         // rotate_slices.cpp:128 writes with stride num_voxels_y.
         out[(uint64_t)k * npix + (uint64_t)x_idx + (uint64_t)y_idx * out_stride_y] = val;
     }
+}
+
+// Launches the rotation of every slice of g on st; slices go in chunks of
+// at most 65535 (the grid's z limit), each chunk with its own base pointers.
+cudaError_t launch_rotate(cudaStream_t st, const ctbb_geom_c& g, const float* in, float* out, const double* cs) {
+    const uint64_t npix = g.num_voxels_x * g.num_voxels_y;
+    if (npix == 0 || g.num_voxels_z == 0) return cudaSuccess;
+    const unsigned gx = (unsigned)((g.num_voxels_x + kRotBlock * kRotPix - 1) / (kRotBlock * kRotPix));
+    for (uint64_t k0 = 0; k0 < g.num_voxels_z; k0 += 65535) {
+        const unsigned nz = (unsigned)std::min<uint64_t>(65535, g.num_voxels_z - k0);
+        rotate_kernel<<<dim3(gx, (unsigned)g.num_voxels_y, nz), kRotBlock, 0, st>>>(
+            in + k0 * npix, out + k0 * npix, (int)g.num_voxels_x, (int)g.num_voxels_y, (int)nz, (int)g.nx, (int)g.ny,
+            (int)g.num_voxels_y, cs + 2 * k0, g.center_voxel_x, g.center_voxel_y);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 ctbb_status angles(const ctbb_geom_c& g, const double* tube_angles_deg, const uint64_t* slice_indices, int direction,
@@ -84,12 +117,7 @@ ctbb_status rotate_device(ctbb_ctx* ctx, const ctbb_geom_c& g, const double* tub
     cudaStream_t st = ctx->stream;
     cudaError_t e = cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess) {
-        const uint64_t n = g.num_voxels_x * g.num_voxels_y * g.num_voxels_z;
-        const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
-        rotate_kernel<<<grid, 256, 0, st>>>(d_in, d_out, (int)g.num_voxels_x, (int)g.num_voxels_y,
-                                            (int)g.num_voxels_z, (int)g.nx, (int)g.ny, (int)g.num_voxels_y, d_cs,
-                                            g.center_voxel_x, g.center_voxel_y);
-        e = cudaGetLastError();
+        e = launch_rotate(st, g, d_in, d_out, d_cs);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     }
     cudaFree(d_cs);
@@ -193,12 +221,7 @@ extern "C" ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_
     cudaStream_t st = ctx->stream;
     CTBB_CUDA(cudaMemcpyAsync(d_cs, cs.data(), cs.size() * sizeof(double), cudaMemcpyHostToDevice, st));
     const ctbb_geom_c& g = *geom;
-    const uint64_t n = g.num_voxels_x * g.num_voxels_y * g.num_voxels_z;
-    const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((n + 255) / 256, (uint64_t)ctx->sm_count * 16));
-    rotate_kernel<<<grid, 256, 0, st>>>(in_dev, out_dev, (int)g.num_voxels_x, (int)g.num_voxels_y,
-                                        (int)g.num_voxels_z, (int)g.nx, (int)g.ny, (int)g.num_voxels_y, d_cs,
-                                        g.center_voxel_x, g.center_voxel_y);
-    CTBB_CUDA(cudaGetLastError());
+    CTBB_CUDA(launch_rotate(st, g, in_dev, out_dev, d_cs));
     CTBB_CUDA(cudaStreamSynchronize(st));
     return CTBB_OK;
 }

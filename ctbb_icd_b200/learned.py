@@ -62,7 +62,7 @@ class WarmStartNet:
 
     @property
     def set_engine(self, engine: int):
-        """CNN_ENGINE_TCGEN05 (default) or CNN_ENGINE_MMA_SYNC for the 32 -> 32
+        """CNN_ENGINE_TCGEN05 or CNN_ENGINE_MMA_SYNC (default) for the 32 -> 32
         convolutions (ctbb_cnn_set_engine)."""
         check(lib().ctbb_cnn_set_engine(self.handle, int(engine)))
 

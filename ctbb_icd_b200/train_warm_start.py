@@ -47,7 +47,7 @@ def main(argv=None):
     ap.add_argument("--prio-passes", type=int, default=2)
     ap.add_argument("--eval-scans", type=int, default=2)
     ap.add_argument("--pairs", default=None, help="npz cache of the generated pairs (read if present, else written)")
-    ap.add_argument("--engine", choices=["tcgen05", "mma_sync"], default="tcgen05",
+    ap.add_argument("--engine", choices=["tcgen05", "mma_sync"], default="mma_sync",
                     help="tensor-core path of the 32 -> 32 convolutions")
     ap.add_argument("--out", default=None)
     ap.add_argument("--report", default=None)

@@ -493,8 +493,8 @@ typedef struct ctbb_cnn ctbb_cnn;
 ctbb_status ctbb_cnn_create(ctbb_ctx* ctx, int32_t blocks, uint64_t seed, ctbb_cnn** out);
 void ctbb_cnn_free(ctbb_cnn* cnn);
 /* Tensor-core path of the 32 -> 32 convolutions (forward and backward-data):
- * TCGEN05 (default) = tcgen05.mma with a TMEM accumulator and TMA-staged
- * operands; MMA_SYNC = the warp-level mma.sync kernel, kept as a cross-check.
+ * TCGEN05 = tcgen05.mma with a TMEM accumulator and TMA-staged operands;
+ * MMA_SYNC (default) = the warp-level mma.sync kernel.
  * A tcgen05 wait that runs out makes the call return CTBB_ERR_TIMEOUT. */
 enum { CTBB_CNN_ENGINE_MMA_SYNC = 0, CTBB_CNN_ENGINE_TCGEN05 = 1 };
 ctbb_status ctbb_cnn_set_engine(ctbb_cnn* cnn, int32_t engine);
