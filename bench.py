@@ -224,7 +224,8 @@ def run_ours(args, rank, world, dist):
         peak, peak_kind = measured_peak()
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
-        kernel = ("icd_staged_kernel" if opts.stage_column else "icd_grouped_kernel") \
+        kernel = ("icd_lockstep_kernel" if opts.stage_column == 3 else
+                  "icd_staged_kernel" if opts.stage_column else "icd_grouped_kernel") \
             if opts.warps_per_voxel <= 1 else "icd_cta_kernel"
         traffic = read_traffic(kernel)
         out = {
@@ -764,7 +765,8 @@ def main():
                          "batch: 32 uneven scans (config 4)")
     ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
     ap.add_argument("--stage-column", type=int, default=-1,
-                    help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory")
+                    help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory, "
+                         "3 sweeps each slice stack in lockstep in one CTA")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

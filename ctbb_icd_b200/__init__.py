@@ -23,7 +23,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from ._lib import (  # noqa: F401
-    ESTIMATE_FORWARD, ESTIMATE_ZERO, ICD_GROUPED, ICD_SEQUENTIAL, PENALTY_EDGE_PRESERVING, PENALTY_QUADRATIC,
+    CNN_ENGINE_MMA_SYNC, CNN_ENGINE_TCGEN05, ESTIMATE_FORWARD, ESTIMATE_ZERO, ICD_GROUPED, ICD_SEQUENTIAL, PENALTY_EDGE_PRESERVING, PENALTY_QUADRATIC,
     ROTATE_FIXED2ROTATING, ROTATE_ROTATING2FIXED, SSM_BOTH, SSM_FP16, SSM_FP32, CtbbError,
     GeomC, IcdOpts, IterStats, PhantomSpec, PrmStrings, SsmInfo, check, lib, ptr,
 )

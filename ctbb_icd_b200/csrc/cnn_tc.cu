@@ -42,8 +42,9 @@ constexpr int kLine = kM + 2;                   // input voxels per halo line
 // multiple of 128 bytes because a tiled TMA copy must land on a 128-byte
 // aligned shared-memory address.
 constexpr int kChunkBytes = ((kLine * 16 + 127) / 128) * 128;  // 2176
-constexpr int kLineBytes = 4 * kChunkBytes;     // 8320
-constexpr int kHaloBytes = 9 * kLineBytes;      // 74880
+constexpr int kBoxBytes = kLine * 16;           // 2080 bytes land per TMA box
+constexpr int kLineBytes = 4 * kChunkBytes;     // 8704
+constexpr int kHaloBytes = 9 * kLineBytes;      // 78336
 constexpr int kTapWBytes = 4 * kC * 16;         // 2048
 constexpr int kWBytes = kTaps * kTapWBytes;     // 55296
 constexpr int kOffHalo0 = kWBytes;
@@ -155,7 +156,7 @@ __device__ __forceinline__ void issue_halo(const CUtensorMap* map, uint32_t halo
                                            uint64_t t) {
     int x0, y, z;
     tile_coords(d, t, x0, y, z);
-    mbar_expect_tx(bar, (uint32_t)(9 * 4 * kChunkBytes));
+    mbar_expect_tx(bar, (uint32_t)(9 * 4 * kBoxBytes));  // bytes delivered, not the padded stride
 #pragma unroll 1
     for (int line = 0; line < 9; ++line) {
         const int dz = line / 3 - 1, dy = line % 3 - 1;

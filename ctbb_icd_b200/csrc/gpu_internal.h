@@ -87,11 +87,17 @@ struct ctbb_recon {
     uint32_t* d_order = nullptr;
     uint64_t n_order = 0;
     int order_P = 0;
+    // Where each slice stack (same-parity slices of one cell) starts in the
+    // order, n_stacks + 1 entries (the last is n_order).
+    uint32_t* d_stacks = nullptr;
+    uint64_t n_stacks = 0;
     // Learned warm start: per-voxel priority (size of the warm-start step)
     // and the visiting order restricted to the highest-priority voxels.
     float* d_prio = nullptr;
     uint32_t* d_prio_order = nullptr;
     uint64_t n_prio_order = 0;
+    uint32_t* d_prio_stacks = nullptr;
+    uint64_t n_prio_stacks = 0;
     int prio_P = 0;
     // Grouped iteration captured in a CUDA graph, and the launch it encodes.
     cudaGraphExec_t icd_graph = nullptr;

@@ -51,6 +51,7 @@
 
 #include <algorithm>
 #include <cub/cub.cuh>
+#include <thrust/iterator/counting_iterator.h>
 #include <type_traits>
 #include <vector>
 
@@ -315,7 +316,13 @@ __device__ __forceinline__ double penalty_solve(int penalty, double lam, double 
         lo = fmin(lo, __shfl_sync(0xffffffffu, dmin, 0));
         hi = fmax(hi, __shfl_sync(0xffffffffu, dmax, 0));
     }
+    // Newton from beta / alpha, kept inside the bracket: a step that leaves
+    // it, or that would not at least halve the step before last, is replaced
+    // by bisection (Numerical Recipes' rtsafe rule), so every iteration
+    // shrinks the bracket or converges quadratically. A Newton step landing
+    // on the bracket's end is kept (an exact root, f = 0, ends there).
     double c = beta / alpha;
+    double step_old = hi - lo, step = step_old;
     for (int it = 0; it < 64; ++it) {
         const double t = c - diff;
         const double den = del + fabs(t);
@@ -326,7 +333,9 @@ __device__ __forceinline__ double penalty_solve(int penalty, double lam, double 
         else
             lo = c;
         double cn = c - f / fp;
-        if (!(cn > lo && cn < hi)) cn = 0.5 * (lo + hi);
+        if (!(cn >= lo && cn <= hi) || fabs(2.0 * f) > fabs(step_old * fp)) cn = 0.5 * (lo + hi);
+        step_old = step;
+        step = cn - c;
         const bool done = fabs(cn - c) <= 1e-12 * (1e-3 + fabs(c)) || (hi - lo) <= 1e-14;
         c = cn;
         if (done) break;
@@ -461,6 +470,148 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
         const unsigned long long before = n_ent;
         process_item<WT, U>(P, order, colptr, vptr, idx, w, start, e, x, item, lane, &n_ent);
         n_upd += n_ent != before;
+    }
+    flush_counts(stats, n_upd, n_ent, lane);
+}
+
+// Entries p0, p0+32, ..., p0+32(U-1) of an item's entry sequence: positions
+// [0, n1) are matrix entries [mid, en) (the stack's common start view to the
+// end of the slice's window), positions [n1, n) entries [b, mid); hi = mid,
+// lo = b - n1, so entry = position + (position < n1 ? hi : lo).
+template <int U, class WT>
+__device__ __forceinline__ void load_seq(const int32_t* __restrict__ idx, const WT* __restrict__ w, int p0, int n,
+                                         int n1, int64_t hi, int64_t lo, int off, uint64_t pol, int* q, float* wt) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int p = p0 + 32 * u;
+        if (p < n) {
+            const int64_t m = (int64_t)p + (p < n1 ? hi : lo);
+            q[u] = ld_idx(idx + m, pol) + off;
+            wt[u] = ldw_hint(w, m, pol);
+        } else {
+            q[u] = -1;
+            wt[u] = 0.f;
+        }
+    }
+}
+
+// Lockstep stacks: one CTA of kStack warps per slice stack (the same-parity
+// slices of one physical cell, consecutive in the visiting order; the stack
+// table lists where each starts). Members start at the stack's common data
+// view and wrap around (as in process_item), so at equal positions of their
+// entry sequences they are at about the same data view; a CTA barrier after
+// every chunk of 32 x U entries keeps them within a chunk of one another, so
+// the sinogram sectors they share are fetched from DRAM once and hit in L2
+// for the others (items of one stack drifting apart by more than the L2's
+// residence time was what made the streamed kernel re-read them). The
+// scatter walks the chunks back in the same lockstep.
+template <class WT, int U>
+__global__ void __launch_bounds__(32 * kStack, U == 8 ? 2 : 1) icd_lockstep_kernel(
+    GParams P, const uint32_t* __restrict__ order, const uint32_t* __restrict__ stacks, uint64_t n_stacks,
+    const int64_t* __restrict__ colptr, const uint32_t* __restrict__ vptr, const int32_t* __restrict__ idx,
+    const WT* __restrict__ w, const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue,
+    unsigned long long* stats) {
+    __shared__ unsigned long long s_stack;
+    __shared__ int s_chunks[kStack];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    unsigned long long n_ent = 0, n_upd = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_stack = atomicAdd(queue, 1ull);
+        __syncthreads();
+        const unsigned long long sid = s_stack;
+        if (sid >= n_stacks) break;
+        const uint32_t i0 = __ldg(stacks + sid), i1 = __ldg(stacks + sid + 1);
+        // A stack holds at most kStack items; longer runs go in blocks.
+        for (uint32_t j0 = i0; j0 < i1; j0 += kStack) {
+            const uint32_t item = j0 + (uint32_t)wid;
+            int64_t hi = 0, lo = 0, q = 0;
+            int n = 0, n1 = 0, off = 0;
+            if (item < i1) {
+                const uint32_t packed = __ldg(order + item);
+                const uint64_t col = packed / (uint32_t)P.nz;
+                const int k = (int)(packed % (uint32_t)P.nz);
+                q = (int64_t)col + (int64_t)ncol * k;
+                const int s = start[k];
+                const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+                if (v1 > v0) {
+                    const int64_t cb = colptr[col];
+                    const uint32_t* vp = vptr + col * P.nvsm1;
+                    const uint32_t b = vp[v0], en = vp[v1];
+                    const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1),
+                                       ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
+                    const uint32_t mid = vp[min(max(start[kl] - s, v0), v1)];
+                    n = (int)(en - b);
+                    n1 = (int)(en - mid);
+                    hi = cb + mid;
+                    lo = cb + b - n1;
+                }
+                off = s * P.nch * P.nr;
+            }
+            const int chunks = (n + 32 * U - 1) / (32 * U);
+            if (lane == 0) s_chunks[wid] = chunks;
+            __syncthreads();
+            int maxc = 0;
+#pragma unroll
+            for (int i = 0; i < kStack; ++i) maxc = max(maxc, s_chunks[i]);
+            // (maxc is the same in every warp.) With no chunk loop below,
+            // this barrier keeps s_chunks from being rewritten while read.
+            if (maxc == 0) __syncthreads();
+
+            float acc_b = 0.f, acc_a = 0.f;
+            {
+                const uint64_t keep = l2_keep();
+                int qa[U];
+                float wa[U];
+                load_seq<U>(idx, w, lane, n, n1, hi, lo, off, keep, qa, wa);
+                for (int c = 0; c < maxc; ++c) {
+                    if (c < chunks) {
+                        float ev[U];
+#pragma unroll
+                        for (int u = 0; u < U; ++u) ev[u] = (qa[u] >= 0) ? __ldcg(e + qa[u]) : 0.f;
+                        int qb[U];
+                        float wb[U];
+                        load_seq<U>(idx, w, (c + 1) * (32 * U) + lane, n, n1, hi, lo, off, keep, qb, wb);
+#pragma unroll
+                        for (int u = 0; u < U; ++u) {
+                            acc_b = fmaf(wa[u], ev[u], acc_b);
+                            acc_a = fmaf(wa[u], wa[u], acc_a);
+                            qa[u] = qb[u];
+                            wa[u] = wb[u];
+                        }
+                    }
+                    __syncthreads();
+                }
+            }
+            float du = 0.f;
+            if (item < i1) {
+                const double beta = (double)warp_sum(acc_b);
+                const double alpha = (double)warp_sum(acc_a);
+                const double xq = (double)__ldcg(x + q);
+                double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+                if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+                if (lane == 0) x[q] = (float)(xq + upd);
+                du = (float)upd;
+            }
+            {
+                const uint64_t drop = l2_drop();
+                for (int c = maxc - 1; c >= 0; --c) {
+                    if (du != 0.f && c < chunks) {
+                        int qs[U];
+                        float ws[U];
+                        load_seq<U>(idx, w, c * (32 * U) + lane, n, n1, hi, lo, off, drop, qs, ws);
+#pragma unroll
+                        for (int u = 0; u < U; ++u)
+                            if (qs[u] >= 0) atomicAdd(e + qs[u], -du * ws[u]);
+                    }
+                    __syncthreads();
+                }
+            }
+            if (du != 0.f) {
+                n_ent += (unsigned long long)n;
+                ++n_upd;
+            }
+        }
     }
     flush_counts(stats, n_upd, n_ent, lane);
 }
@@ -800,6 +951,21 @@ __global__ void split_collisions_kernel(const uint64_t* __restrict__ sorted, uin
     }
 }
 
+// Slice stacks of the sorted order: a stack is a run of items with the same
+// key apart from the slice, and the same block of 2 kStack slices (kStack
+// slices of one parity). flags[p] = 1 where a stack starts.
+__global__ void stack_heads_kernel(const uint64_t* __restrict__ sorted, uint64_t n, uint64_t nz,
+                                   uint8_t* __restrict__ flags) {
+    for (uint64_t p = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; p < n; p += (uint64_t)gridDim.x * blockDim.x) {
+        bool head = p == 0;
+        if (!head) {
+            const uint64_t a = sorted[p - 1], b = sorted[p];
+            head = a / nz != b / nz || (a % nz) / (2 * kStack) != (b % nz) / (2 * kStack);
+        }
+        flags[p] = head ? 1 : 0;
+    }
+}
+
 // Sum of in-range entries over (column inside the FOV, slice): the unit of
 // work of one iteration. One warp per column.
 __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uint32_t* __restrict__ vptr,
@@ -874,8 +1040,12 @@ uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     // The staged kernel keeps one CTA of 4 (or 8) updates per SM (its stage
     // fills the SM's shared memory).
     const int staged = rc->ctx->sm_count * (o.stage_column == 2 ? 8 : 4);
+    // The lockstep kernel keeps two CTAs of kStack updates per SM with 8
+    // entries per lane in flight (one with 16).
+    const int lockstep = rc->ctx->sm_count * (o.entries_per_lane == 16 ? 1 : 2) * kStack;
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight
-                                        : (o.stage_column ? staged : default_warps_in_flight(rc));
+                  : o.stage_column == 3 ? lockstep
+                  : (o.stage_column ? staged : default_warps_in_flight(rc));
     const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     return std::max<uint64_t>(1, (uint64_t)(W / wpv));
 }
@@ -903,7 +1073,7 @@ using namespace ctbb;
 // Visiting order for tile edge P_lat, optionally restricted to the voxels
 // whose priority is at least thr.
 ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float thr, uint32_t** out,
-                             uint64_t* n_out) {
+                             uint64_t* n_out, uint32_t** stacks_out, uint64_t* n_stacks_out) {
     using namespace ctbb;
     const ctbb_geom_c& g = rc->geom;
     ctbb_ctx* ctx = rc->ctx;
@@ -994,15 +1164,56 @@ ctbb_status build_order_into(ctbb_recon* rc, int P_lat, const float* prio, float
             hi = lo;
         }
     }
+    // Stack table: where each slice stack starts in the order, then n_valid.
+    uint32_t* d_st = nullptr;
+    uint64_t n_st = 0;
+    if (e == cudaSuccess && stacks_out) {
+        uint8_t* d_flags = nullptr;
+        int* d_num = nullptr;
+        void* d_tmp2 = nullptr;
+        size_t tmp2 = 0;
+        e = cudaMalloc(&d_st, (n_valid + 1) * sizeof(uint32_t));
+        if (e == cudaSuccess && n_valid > 0) {
+            e = cudaMalloc(&d_flags, n_valid);
+            if (e == cudaSuccess) e = cudaMalloc(&d_num, sizeof(int));
+            if (e == cudaSuccess) {
+                const int grid =
+                    (int)std::max<uint64_t>(1, std::min<uint64_t>((n_valid + 255) / 256, (uint64_t)ctx->sm_count * 16));
+                stack_heads_kernel<<<grid, 256, 0, st>>>(d_k1, n_valid, (uint64_t)O.nz, d_flags);
+                e = cudaGetLastError();
+            }
+            const thrust::counting_iterator<uint32_t> pos(0);
+            if (e == cudaSuccess)
+                e = cub::DeviceSelect::Flagged(nullptr, tmp2, pos, d_flags, d_st, d_num, (int)n_valid, st);
+            if (e == cudaSuccess) e = cudaMalloc(&d_tmp2, tmp2);
+            if (e == cudaSuccess)
+                e = cub::DeviceSelect::Flagged(d_tmp2, tmp2, pos, d_flags, d_st, d_num, (int)n_valid, st);
+            int h_num = 0;
+            if (e == cudaSuccess) e = cudaMemcpyAsync(&h_num, d_num, sizeof(int), cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            n_st = (uint64_t)h_num;
+        }
+        const uint32_t nv = (uint32_t)n_valid;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_st + n_st, &nv, sizeof(uint32_t), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        cudaFree(d_flags);
+        cudaFree(d_num);
+        cudaFree(d_tmp2);
+    }
     if (e != cudaSuccess) {
         rcode = fail(e == cudaErrorMemoryAllocation ? CTBB_ERR_OOM : CTBB_ERR_CUDA, "visiting order: %s",
                      cudaGetErrorString(e));
         cudaFree(d_v1);
+        cudaFree(d_st);
         cleanup();
         return rcode;
     }
     *out = d_v1;
     *n_out = n_valid;
+    if (stacks_out) {
+        *stacks_out = d_st;
+        *n_stacks_out = n_st;
+    }
     cleanup();
     return CTBB_OK;
 }
@@ -1034,6 +1245,7 @@ ctbb_status launch_staged(const GParams& P, const uint32_t* order, const ctbb_ss
 struct GraphKey {
     GParams P;
     const void* order;
+    const void* stacks;
     const void* w;
     const void* idx;
     const float* e;
@@ -1046,12 +1258,15 @@ struct GraphKey {
 // Build (or reuse) the full visiting order for tile edge P_lat.
 ctbb_status build_order(ctbb_recon* rc, int P_lat) {
     if (rc->d_order && rc->order_P == P_lat) return CTBB_OK;
-    uint32_t* o = nullptr;
-    uint64_t n = 0;
-    CTBB_TRY(build_order_into(rc, P_lat, nullptr, 0.f, &o, &n));
+    uint32_t *o = nullptr, *stk = nullptr;
+    uint64_t n = 0, n_stk = 0;
+    CTBB_TRY(build_order_into(rc, P_lat, nullptr, 0.f, &o, &n, &stk, &n_stk));
     cudaFree(rc->d_order);
+    cudaFree(rc->d_stacks);
     rc->d_order = o;
     rc->n_order = n;
+    rc->d_stacks = stk;
+    rc->n_stacks = n_stk;
     rc->order_P = P_lat;
     return CTBB_OK;
 }
@@ -1122,8 +1337,12 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     if (wpv != 1 && wpv != 4 && wpv != 8)
         return fail(CTBB_ERR_INVALID_ARG, "warps_per_voxel must be 1, 4 or 8 (got %d)", wpv);
     const int stage = o.stage_column;
-    if (stage < 0 || stage > 2) return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0, 1 or 2 (got %d)", stage);
+    if (stage < 0 || stage > 3)
+        return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0, 1, 2 or 3 (got %d)", stage);
     if (stage && wpv != 1) return fail(CTBB_ERR_INVALID_ARG, "stage_column needs one warp per voxel update");
+    const uint32_t* stacks = prio ? rc->d_prio_stacks : rc->d_stacks;
+    const uint64_t n_stacks = prio ? rc->n_prio_stacks : rc->n_stacks;
+    if (stage == 3 && !stacks) return fail(CTBB_ERR_INVALID_ARG, "visiting order has no stack table");
     const int epl = o.entries_per_lane > 0 ? o.entries_per_lane : kU;
     if (epl != 8 && epl != 16) return fail(CTBB_ERR_INVALID_ARG, "entries_per_lane must be 8 or 16 (got %d)", epl);
     ctbb_ctx* ctx = rc->ctx;
@@ -1139,6 +1358,33 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     // persistent kernel (prepare: only the launch attributes, no work).
     auto issue = [&](cudaStream_t s, bool prepare) -> ctbb_status {
         if (!prepare) CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned long long), s));
+        if (stage == 3) {
+            if (prepare) return CTBB_OK;
+            // One CTA (kStack warps) per stack: at most in_flight / kStack
+            // stacks in flight keeps within the order's concurrency bound.
+            const int blocks = (int)std::max<uint64_t>(1, in_flight / kStack);
+            if (epl == 16) {
+                if (h)
+                    icd_lockstep_kernel<__half, 16><<<blocks, 32 * kStack, 0, s>>>(
+                        P, order, stacks, n_stacks, cp, vp, ix, ssm->d_w16, rc->d_start, rc->d_e32, rc->d_x32,
+                        ctx->d_queue, stats);
+                else
+                    icd_lockstep_kernel<float, 16><<<blocks, 32 * kStack, 0, s>>>(
+                        P, order, stacks, n_stacks, cp, vp, ix, ssm->d_w32, rc->d_start, rc->d_e32, rc->d_x32,
+                        ctx->d_queue, stats);
+            } else {
+                if (h)
+                    icd_lockstep_kernel<__half, 8><<<blocks, 32 * kStack, 0, s>>>(
+                        P, order, stacks, n_stacks, cp, vp, ix, ssm->d_w16, rc->d_start, rc->d_e32, rc->d_x32,
+                        ctx->d_queue, stats);
+                else
+                    icd_lockstep_kernel<float, 8><<<blocks, 32 * kStack, 0, s>>>(
+                        P, order, stacks, n_stacks, cp, vp, ix, ssm->d_w32, rc->d_start, rc->d_e32, rc->d_x32,
+                        ctx->d_queue, stats);
+            }
+            CTBB_CUDA(cudaGetLastError());
+            return CTBB_OK;
+        }
         if (stage) {
             // stage_column 1: 4 warps (updates) per CTA, 2: 8 (half the stage each).
             if (stage == 1) {
@@ -1201,6 +1447,7 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     memset(&key, 0, sizeof(key));
     key.P = P;
     key.order = order;
+    key.stacks = stacks;
     key.w = h ? (const void*)ssm->d_w16 : (const void*)ssm->d_w32;
     key.idx = ix;
     key.e = rc->d_e32;
@@ -1553,10 +1800,15 @@ extern "C" ctbb_status ctbb_gpu_recon_set_priority(ctbb_recon* rc, const ctbb_ic
     uint32_t* order = nullptr;
     uint64_t n_order = 0;
     const int T = lattice_spacing(rc, o);
-    CTBB_TRY(build_order_into(rc, T, rc->d_prio, thr, &order, &n_order));
+    uint32_t* stk = nullptr;
+    uint64_t n_stk = 0;
+    CTBB_TRY(build_order_into(rc, T, rc->d_prio, thr, &order, &n_order, &stk, &n_stk));
     cudaFree(rc->d_prio_order);
+    cudaFree(rc->d_prio_stacks);
     rc->d_prio_order = order;
     rc->n_prio_order = n_order;
+    rc->d_prio_stacks = stk;
+    rc->n_prio_stacks = n_stk;
     rc->prio_P = T;
     return CTBB_OK;
 }

@@ -316,8 +316,10 @@ extern "C" void ctbb_gpu_recon_free(ctbb_recon* rc) {
     cudaFree(rc->d_x64);
     cudaFree(rc->d_x32);
     cudaFree(rc->d_order);
+    cudaFree(rc->d_stacks);
     cudaFree(rc->d_prio);
     cudaFree(rc->d_prio_order);
+    cudaFree(rc->d_prio_stacks);
     if (rc->icd_graph) cudaGraphExecDestroy(rc->icd_graph);
     ctx_release(rc->ctx);
     delete rc;
@@ -611,7 +613,10 @@ extern "C" ctbb_status ctbb_gpu_recon_warm_start(ctbb_recon* rc, const ctbb_ssm*
     cudaFree(d_a);
     cudaFree(d_b);
     cudaFree(rc->d_prio_order);
+    cudaFree(rc->d_prio_stacks);
     rc->d_prio_order = nullptr;
     rc->n_prio_order = 0;
+    rc->d_prio_stacks = nullptr;
+    rc->n_prio_stacks = 0;
     return st;
 }

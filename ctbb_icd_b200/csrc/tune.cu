@@ -48,8 +48,8 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     if (copy(d_xs, rc->d_x32, d_es, rc->d_e32) != cudaSuccess) status = fail(CTBB_ERR_CUDA, "autotune snapshot copy");
 
     // Candidates (warps per voxel, warps in flight, entries per lane, tile
-    // edge, column stage): the shared-memory staged kernel with 4 or 8
-    // updates per SM; one warp per voxel streaming the column twice at
+    // edge, column stage): the lockstep stack kernel; the shared-memory
+    // staged kernel with 4 or 8 updates per SM; one warp per voxel streaming the column twice at
     // 1/4 .. 2 times the coupling-bound default; 8 or 16 entries per lane in
     // flight, the default tile edge for that concurrency (and half of it);
     // 4 warps per voxel with four updates per SM. Launches cap the updates in
@@ -62,8 +62,12 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
         int wpv, w, epl, half, stage;
     };
     std::vector<Cand> cands;
-    // Shared-memory staged kernels first: one CTA per SM with 4 (or 8)
-    // updates, the matrix read once per update.
+    // Lockstep stacks first: two CTAs of 16 updates per SM with 8 entries per
+    // lane in flight, one CTA with 16.
+    cands.push_back({1, 2 * 16 * sms, 8, 0, 3});
+    cands.push_back({1, 16 * sms, 16, 0, 3});
+    // Shared-memory staged kernels: one CTA per SM with 4 (or 8) updates,
+    // the matrix read once per update.
     for (int epl : {16, 8}) {
         cands.push_back({1, 4 * sms, epl, 0, 1});
         cands.push_back({1, 8 * sms, epl, 0, 2});

@@ -60,12 +60,12 @@ class WarmStartNet:
         self.handle = h
         self.set_scaling(S_IN, S_OUT)
 
-    @property
     def set_engine(self, engine: int):
         """CNN_ENGINE_TCGEN05 or CNN_ENGINE_MMA_SYNC (default) for the 32 -> 32
         convolutions (ctbb_cnn_set_engine)."""
         check(lib().ctbb_cnn_set_engine(self.handle, int(engine)))
 
+    @property
     def n_params(self) -> int:
         return int(lib().ctbb_cnn_num_params(self.handle))
 

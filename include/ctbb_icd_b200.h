@@ -292,7 +292,12 @@ typedef struct ctbb_icd_opts {
                                  matrix entries from HBM for the gather and again
                                  for the scatter; 1 keeps them in a shared-memory
                                  stage between the two (4 updates per CTA), 2 the
-                                 same with 8 updates per CTA and half the stage   */
+                                 same with 8 updates per CTA and half the stage;
+                                 3 runs each slice stack (up to 16 same-parity
+                                 slices at one physical cell) as one CTA whose
+                                 warps sweep the stack's data views in lockstep,
+                                 so the sinogram sectors they share are fetched
+                                 from HBM once                                     */
 } ctbb_icd_opts;
 
 /*
@@ -442,11 +447,13 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
 /*
  * Autotuner for grouped ICD (no reference counterpart). From the current
  * iterate, runs probe_iters iterations for each candidate (warps per voxel,
- * warps in flight, entries per lane, tile edge of the visiting order) and
- * keeps the one with the
+ * warps in flight, entries per lane, tile edge of the visiting order, column
+ * schedule) and keeps the one with the
  * largest decrease of the FP64 cost per millisecond of device time. The
- * iterate and e are restored afterwards; *best = *base with the four fields
- * set. Candidates: one warp per voxel at 1/4, 1/2, 1 and 2 times the
+ * iterate and e are restored afterwards; *best = *base with those fields
+ * set. Candidates: the lockstep stack kernel (stage_column 3) with 8 or 16
+ * entries per lane; the shared-memory staged kernel (stage_column 1, 2);
+ * one warp per voxel at 1/4, 1/2, 1 and 2 times the
  * coupling-bound default of warps in flight, with 8 or 16 entries per lane
  * in flight and the default tile edge for that concurrency (half of it too
  * at the default); 4 warps per voxel with four updates per SM.

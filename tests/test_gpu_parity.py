@@ -33,7 +33,8 @@ def test_ssm_matches_reference_matrix_bin(golden, ctx, tmp_path):
     assert np.array_equal(m.idx, golden.idx)
     assert np.array_equal(m.w.view(np.int32), golden.w.view(np.int32))
     info = ssm.info()
-    assert info.nnz == golden.colptr[-1] and info.ffs == int(golden.rp.geom.Phiffs)
+    assert info.nnz == golden.colptr[-1]
+    assert info.ffs == int(bool(golden.rp.geom.Phiffs or golden.rp.geom.Zffs))  # in-plane and/or z spot
 
 
 def test_ssm_matches_port(wl, ctx):
@@ -197,7 +198,8 @@ def converged_cfg1_small(ctx, tmp_path_factory):
 
 
 @pytest.mark.parametrize("weights,wpv,stage", [(C.SSM_FP32, 1, 0), (C.SSM_FP16, 1, 0), (C.SSM_FP32, 8, 0),
-                                               (C.SSM_FP16, 4, 0), (C.SSM_FP16, 1, 1), (C.SSM_FP32, 1, 2)])
+                                               (C.SSM_FP16, 4, 0), (C.SSM_FP16, 1, 1), (C.SSM_FP32, 1, 2),
+                                               (C.SSM_FP16, 1, 3), (C.SSM_FP32, 1, 3)])
 def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage):
     rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
     rc = C.Recon(rp, data.slice_indices, ctx)
@@ -278,7 +280,7 @@ def converged_small_ffs(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1)])
+@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1), (C.SSM_FP16, 3)])
 def test_grouped_edge_preserving_reaches_converged_cost(ctx, converged_small_ffs, weights, stage):
     rp, data, ssm, x_ref, cost_ref = converged_small_ffs
     rc = C.Recon(rp, data.slice_indices, ctx)
