@@ -406,6 +406,10 @@ def _stage_batch(args, C, ctx, torch, clocks):
     while pending:
         scans = []
         while pending:
+            # Leave room for the iteration's own buffers (graph, FP64
+            # refresh of the largest scan) before packing another scan.
+            if scans and torch.cuda.mem_get_info()[0] < 4 * 2 ** 30:
+                break
             i = pending[0]
             sp = specs[i]
             d = os.path.join(workdir, sp["name"])
@@ -499,6 +503,8 @@ def _stage_cnn(args, C, ctx, torch, clocks):
 
     shape = args.cnn_shape
     net = L.WarmStartNet(ctx, 4, seed=0)
+    engine = C.CNN_ENGINE_TCGEN05 if args.cnn_engine == "tcgen05" else C.CNN_ENGINE_MMA_SYNC
+    net.set_engine(engine)
     g = torch.Generator(device="cuda").manual_seed(0)
     x = (0.15 + 0.1 * torch.rand(*shape, device="cuda", generator=g)).contiguous()
     xc = (x + 0.002 * torch.randn(*shape, device="cuda", generator=g)).contiguous()
@@ -532,10 +538,11 @@ def _stage_cnn(args, C, ctx, torch, clocks):
     return {"metric": "network voxels/s", "value": nvox / (fwd_ms / 1e3), "unit": "voxels/s",
             "ms_per_step": fwd_ms, "dtype": "bf16 operands, fp32 accumulation",
             "config": {"workload": f"warm-start CNN forward, 4 residual blocks x 32 channels, volume {shape}",
-                       "stage": "cnn", "train_step_ms": train_ms,
+                       "stage": "cnn", "engine": args.cnn_engine, "train_step_ms": train_ms,
                        "train_conv_tflops": 6 * 4 * conv_flop / (train_ms / 1e3) / 1e12},
             "roofline": {"bound": "tensor", "achieved": fwd_tflops, "peak": peak, "unit": "TFLOP/s",
-                         "frac": fwd_tflops / peak if peak else None, "kernel": "conv_mid_kernel",
+                         "frac": fwd_tflops / peak if peak else None,
+                         "kernel": "conv_mid_tc_kernel" if args.cnn_engine == "tcgen05" else "conv_mid_kernel",
                          "algorithmic_flops_per_pass": 2 * 4 * conv_flop,
                          "peak_source": "measured" if peak else None}}
 
@@ -764,6 +771,8 @@ def main():
                          "slice rotation of the same workload on their own; cnn: the warm-start network; "
                          "batch: 32 uneven scans (config 4)")
     ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
+    ap.add_argument("--cnn-engine", choices=["tcgen05", "mma_sync"], default="tcgen05",
+                    help="--stage cnn: tensor-core path of the 32 -> 32 convolutions")
     ap.add_argument("--stage-column", type=int, default=-1,
                     help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory, "
                          "3 sweeps each slice stack in lockstep in one CTA")

@@ -18,6 +18,8 @@
 #include <string>
 #include <vector>
 
+#include <cuda_runtime_api.h>
+
 #include "common.h"
 #include "phantom.h"
 
@@ -43,6 +45,9 @@ ctbb_status fail(ctbb_status st, const char* fmt, ...) {
     vsnprintf(buf, sizeof(buf), fmt, ap);
     va_end(ap);
     g_last_error = buf;
+    // A failed allocation is reported here; the CUDA runtime would otherwise
+    // keep it as its last error and a later launch check would return it.
+    if (st == CTBB_ERR_OOM) cudaGetLastError();
     return st;
 }
 

@@ -1043,9 +1043,14 @@ uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     // The lockstep kernel keeps two CTAs of kStack updates per SM with 8
     // entries per lane in flight (one with 16).
     const int lockstep = rc->ctx->sm_count * (o.entries_per_lane == 16 ? 1 : 2) * kStack;
+    // Unless the caller sets the count, the coupling bound (default_warps_in_
+    // flight) caps every kernel: on a small volume a CTA-shaped default would
+    // put a large share of the voxels on each ray in flight at once, and the
+    // edge-preserving iteration then oscillates.
+    const int coupling = default_warps_in_flight(rc);
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight
-                  : o.stage_column == 3 ? lockstep
-                  : (o.stage_column ? staged : default_warps_in_flight(rc));
+                  : o.stage_column == 3 ? std::min(lockstep, coupling)
+                  : (o.stage_column ? std::min(staged, coupling) : coupling);
     const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     return std::max<uint64_t>(1, (uint64_t)(W / wpv));
 }
