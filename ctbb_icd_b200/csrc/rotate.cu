@@ -31,6 +31,14 @@ namespace {
 constexpr int kTile = 32, kRows = 8, kRotPix = kTile / kRows;
 constexpr int kBoxCap = 52 * 52;  // floats; a larger box (never for kTile 32) reads from global
 
+// FLOAT_CENTRE: the centre (cvx, cvy) is exactly a float. Then
+// (float)((double)xp + cvx) equals the float sum xp + (float)cvx: the exact
+// sum of two floats fits in a double's 53 bits unless the smaller one is
+// below about 2^-29 of the larger, and then it is far below half a float ulp
+// of the larger, so both roundings return the larger. The float add saves
+// two conversions per coordinate (they run on the narrow conversion pipe
+// that bounds this kernel).
+template <bool FLOAT_CENTRE>
 __global__ void __launch_bounds__(kTile * kRows) rotate_kernel(const float* __restrict__ in, float* __restrict__ out,
                                                                int nx, int ny, int nz, int dim1, int dim2,
                                                                int out_stride_y, const double* __restrict__ cs,
@@ -54,14 +62,17 @@ __global__ void __launch_bounds__(kTile * kRows) rotate_kernel(const float* __re
     int f1s[kRotPix], f2s[kRotPix];
     bool inside[kRotPix];
     int lo1 = INT_MAX, hi1 = INT_MIN, lo2 = INT_MAX, hi2 = INT_MIN;
+    const double x = x_idx - cvx;
+    const double cx = c * x, sx = s * x;
+    const float cvx_f = (float)cvx, cvy_f = (float)cvy;
 #pragma unroll
     for (int u = 0; u < kRotPix; ++u) {
         const int y_idx = blockIdx.y * kTile + ty + u * kRows;
-        const double x = x_idx - cvx, y = y_idx - cvy;
-        const float xp = (float)(c * x - s * y);
-        const float yp = (float)(s * x + c * y);
-        const float i1 = (float)((double)xp + cvx);
-        const float i2 = (float)((double)yp + cvy);
+        const double y = y_idx - cvy;
+        const float xp = (float)(cx - s * y);
+        const float yp = (float)(sx + c * y);
+        const float i1 = FLOAT_CENTRE ? __fadd_rn(xp, cvx_f) : (float)((double)xp + cvx);
+        const float i2 = FLOAT_CENTRE ? __fadd_rn(yp, cvy_f) : (float)((double)yp + cvy);
         // interp.h:57-58: zero outside [0, n-2] in either index.
         inside[u] = x_idx < nx && y_idx < ny &&
                     !(i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0));
@@ -76,7 +87,14 @@ __global__ void __launch_bounds__(kTile * kRows) rotate_kernel(const float* __re
             hi2 = max(hi2, f2s[u] + 1);
         }
     }
-    if (lo1 <= hi1) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo1 = min(lo1, __shfl_xor_sync(0xffffffffu, lo1, o));
+        hi1 = max(hi1, __shfl_xor_sync(0xffffffffu, hi1, o));
+        lo2 = min(lo2, __shfl_xor_sync(0xffffffffu, lo2, o));
+        hi2 = max(hi2, __shfl_xor_sync(0xffffffffu, hi2, o));
+    }
+    if ((threadIdx.x & 31) == 0 && lo1 <= hi1) {
         atomicMin(&s_lim[0], lo1);
         atomicMax(&s_lim[1], hi1);
         atomicMin(&s_lim[2], lo2);
@@ -130,7 +148,9 @@ cudaError_t launch_rotate(cudaStream_t st, const ctbb_geom_c& g, const float* in
     const unsigned gy = (unsigned)((g.num_voxels_y + kTile - 1) / kTile);
     for (uint64_t k0 = 0; k0 < g.num_voxels_z; k0 += 65535) {
         const unsigned nz = (unsigned)std::min<uint64_t>(65535, g.num_voxels_z - k0);
-        rotate_kernel<<<dim3(gx, gy, nz), kTile * kRows, 0, st>>>(
+        const bool fc = (double)(float)g.center_voxel_x == g.center_voxel_x &&
+                        (double)(float)g.center_voxel_y == g.center_voxel_y;
+        (fc ? rotate_kernel<true> : rotate_kernel<false>)<<<dim3(gx, gy, nz), kTile * kRows, 0, st>>>(
             in + k0 * npix, out + k0 * npix, (int)g.num_voxels_x, (int)g.num_voxels_y, (int)nz, (int)g.nx, (int)g.ny,
             (int)g.num_voxels_y, cs + 2 * k0, g.center_voxel_x, g.center_voxel_y);
         const cudaError_t e = cudaGetLastError();
