@@ -207,7 +207,13 @@ def run_ours(args, rank, world, dist):
     # scatters nothing), the matrix read once (index + weight), image r+w.
     gathered = st.entries / max(1, st.iterations)
     scattered = st.entries_scattered / max(1, st.iterations)
-    b_iter = 4.0 * gathered + 4.0 * scattered + (4 + w_bytes) * float(info.nnz) + 8.0 * nvox
+    # The matrix in the form the kernel reads: entry pairs (8 B per pair of
+    # rows) when the iteration used them, else index + weight per entry.
+    n_pairs = int(ssm.info().n_pairs)
+    uses_pairs = (n_pairs > 0 and weights_fmt == C.SSM_FP16 and opts.warps_per_voxel > 1
+                  and opts.entry_pairs == 0)
+    ssm_read = 8.0 * n_pairs if uses_pairs else (4 + w_bytes) * float(info.nnz)
+    b_iter = 4.0 * gathered + 4.0 * scattered + ssm_read + 8.0 * nvox
 
     e2e = None
     if args.e2e:
@@ -226,7 +232,7 @@ def run_ours(args, rank, world, dist):
         value = world * nvox * args.steps / (t_max / 1e3)
         kernel = ("icd_lockstep_kernel" if opts.stage_column == 3 else
                   "icd_staged_kernel" if opts.stage_column else "icd_grouped_kernel") \
-            if opts.warps_per_voxel <= 1 else "icd_cta_kernel"
+            if opts.warps_per_voxel <= 1 else ("icd_cta_pairs_kernel" if uses_pairs else "icd_cta_kernel")
         traffic = read_traffic(kernel)
         out = {
             "metric": "voxel-updates/s",
@@ -247,6 +253,8 @@ def run_ours(args, rank, world, dist):
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
                 "scattered_entries_per_iter": scattered, "stage_column": int(opts.stage_column),
+                "matrix_read_as": (f"{n_pairs} entry pairs (8 B each)" if uses_pairs
+                                   else f"entries ({4 + w_bytes} B each)"),
                 "warps_in_flight": opts.warps_in_flight or "auto", "warps_per_voxel": max(1, opts.warps_per_voxel),
                 "entries_per_lane": opts.entries_per_lane or 8,
                 "lattice": opts.lattice or "auto", "autotune": tune,
@@ -771,7 +779,7 @@ def main():
                          "slice rotation of the same workload on their own; cnn: the warm-start network; "
                          "batch: 32 uneven scans (config 4)")
     ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
-    ap.add_argument("--cnn-engine", choices=["tcgen05", "mma_sync"], default="tcgen05",
+    ap.add_argument("--cnn-engine", choices=["tcgen05", "mma_sync"], default="mma_sync",
                     help="--stage cnn: tensor-core path of the 32 -> 32 convolutions")
     ap.add_argument("--stage-column", type=int, default=-1,
                     help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory, "

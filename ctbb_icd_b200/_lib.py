@@ -93,7 +93,7 @@ class PhantomSpec(C.Structure):
 class SsmInfo(C.Structure):
     _fields_ = [
         ("n_columns", _U), ("n_views", _U), ("nnz", _U), ("max_col_nnz", _U),
-        ("bytes_device", _U), ("weights", _I), ("ffs", _I), ("build_ms", _D),
+        ("bytes_device", _U), ("weights", _I), ("ffs", _I), ("build_ms", _D), ("n_pairs", _U),
     ]
 
 
@@ -102,6 +102,7 @@ class IcdOpts(C.Structure):
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
         ("priority", _I), ("warps_per_voxel", _I), ("entries_per_lane", _I), ("stage_column", _I),
+        ("entry_pairs", _I),
     ]
 
 

@@ -58,6 +58,14 @@ struct ctbb_ssm {
     int32_t* d_idx = nullptr;     // [nnz]
     float* d_w32 = nullptr;       // [nnz] (CTBB_SSM_FP32 held)
     __half* d_w16 = nullptr;      // [nnz] (CTBB_SSM_FP16 held)
+    // Entry pairs (built on first use from idx + w16, ssm_build_pairs):
+    // {q, w0 | w1 << 16} for two entries at consecutive sinogram indices,
+    // w1 = 0 for a lone entry; same column / per-view offset layout.
+    int64_t* d_pcolptr = nullptr;  // [ncol + 1]
+    uint32_t* d_pvptr = nullptr;   // [ncol * (nvsm + 1)]
+    uint2* d_pairs = nullptr;      // [npairs]
+    uint64_t npairs = 0;
+    bool pairs_checked = false;  // build tried (pairs kept only where they pay)
     int weights = 0;
     int ffs = 0;
     double build_ms = 0.0;
@@ -116,6 +124,7 @@ ctbb_status ensure_partials(ctbb_ctx* ctx, size_t n);
 
 // ssm.cu
 ctbb_status ssm_validate_geometry(const ctbb_geom_c& g);
+ctbb_status ssm_build_pairs(ctbb_ssm* s);
 
 // recon.cu
 ctbb_status recon_to_grouped(ctbb_recon* rc, const ctbb_ssm* ssm);

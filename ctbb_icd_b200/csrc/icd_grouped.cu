@@ -495,6 +495,156 @@ __device__ __forceinline__ void load_seq(const int32_t* __restrict__ idx, const 
     }
 }
 
+// One voxel update per CTA of WPV warps over the matrix's entry pairs
+// ({q, w0 | w1 << 16}: rows q and q + 1 of one (view, channel), w1 = 0 for a
+// lone entry). Each thread keeps R pairs (2R entries) in registers from the
+// gather to the scatter, so a column of up to 2 * 32 * WPV * R entries is
+// read from HBM once; longer columns re-read their tail. Same update as
+// icd_cta_kernel; the entry counts (for the statistics) come from the entry
+// offsets.
+__device__ __forceinline__ float half_lo(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+__device__ __forceinline__ float half_hi(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+
+template <int WPV, int R>
+__global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
+    GParams P, const uint32_t* __restrict__ order, const int64_t* __restrict__ pcolptr,
+    const uint32_t* __restrict__ pvptr, const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
+    const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue, unsigned long long* stats) {
+    constexpr int NT = 32 * WPV;
+    constexpr int64_t CAP = (int64_t)NT * R;
+    unsigned long long n_ent = 0, n_upd = 0;
+    __shared__ unsigned long long s_item;
+    __shared__ float s_red[2 * WPV + 1];
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    for (;;) {
+        if (tid == 0) s_item = atomicAdd(queue, 1ull);
+        __syncthreads();
+        const uint64_t item = s_item;
+        if (item >= P.n_items) break;
+        const uint32_t packed = __ldg(order + item);
+        const uint64_t col = packed / (uint32_t)P.nz;
+        const int k = (int)(packed % (uint32_t)P.nz);
+        const int64_t q = (int64_t)col + (int64_t)ncol * k;
+        const int s = start[k];
+        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+        int64_t b = 0, en = 0, n_entries = 0;
+        if (v1 > v0) {
+            const int64_t cb = pcolptr[col];
+            const uint32_t* vp = pvptr + col * P.nvsm1;
+            b = cb + vp[v0];
+            en = cb + vp[v1];
+            if (tid == 0) n_entries = (int64_t)vptr[col * P.nvsm1 + v1] - (int64_t)vptr[col * P.nvsm1 + v0];
+        }
+        const int off = s * P.nch * P.nr;
+        const int64_t e0 = min(en, b + CAP);
+        int qr[R];
+        uint32_t wr[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int64_t m = b + tid + (int64_t)NT * r;
+            if (m < e0) {
+                const uint2 pr = __ldg(pairs + m);
+                qr[r] = (int)pr.x + off;
+                wr[r] = pr.y;
+            } else {
+                qr[r] = -1;
+                wr[r] = 0u;
+            }
+        }
+        float acc_b = 0.f, acc_a = 0.f;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            float ev0 = 0.f, ev1 = 0.f;
+            if (qr[r] >= 0) {
+                ev0 = __ldcg(e + qr[r]);
+                if (wr[r] >> 16) ev1 = __ldcg(e + qr[r] + 1);
+            }
+            const float w0 = half_lo(wr[r]), w1 = half_hi(wr[r]);
+            acc_b = fmaf(w0, ev0, acc_b);
+            acc_b = fmaf(w1, ev1, acc_b);
+            acc_a = fmaf(w0, w0, acc_a);
+            acc_a = fmaf(w1, w1, acc_a);
+        }
+        for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+            int qo[kU];
+            uint32_t wo[kU];
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const int64_t m = base + tid + (int64_t)NT * u;
+                if (m < en) {
+                    const uint2 pr = __ldg(pairs + m);
+                    qo[u] = (int)pr.x + off;
+                    wo[u] = pr.y;
+                } else {
+                    qo[u] = -1;
+                    wo[u] = 0u;
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                float ev0 = 0.f, ev1 = 0.f;
+                if (qo[u] >= 0) {
+                    ev0 = __ldcg(e + qo[u]);
+                    if (wo[u] >> 16) ev1 = __ldcg(e + qo[u] + 1);
+                }
+                const float w0 = half_lo(wo[u]), w1 = half_hi(wo[u]);
+                acc_b = fmaf(w0, ev0, acc_b);
+                acc_b = fmaf(w1, ev1, acc_b);
+                acc_a = fmaf(w0, w0, acc_a);
+                acc_a = fmaf(w1, w1, acc_a);
+            }
+        }
+        acc_b = warp_sum(acc_b);
+        acc_a = warp_sum(acc_a);
+        if (lane == 0) {
+            s_red[wid] = acc_b;
+            s_red[WPV + wid] = acc_a;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            double beta = 0.0, alpha = 0.0;
+#pragma unroll
+            for (int i = 0; i < WPV; ++i) {
+                beta += (double)s_red[i];
+                alpha += (double)s_red[WPV + i];
+            }
+            const double xq = (double)__ldcg(x + q);
+            double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+            if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+            if (lane == 0) {
+                x[q] = (float)(xq + upd);
+                s_red[2 * WPV] = (float)upd;
+            }
+        }
+        __syncthreads();
+        const float du = s_red[2 * WPV];
+        if (du != 0.f) {
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                if (qr[r] >= 0) {
+                    atomicAdd(e + qr[r], -du * half_lo(wr[r]));
+                    if (wr[r] >> 16) atomicAdd(e + qr[r] + 1, -du * half_hi(wr[r]));
+                }
+            for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int64_t m = base + tid + (int64_t)NT * u;
+                    if (m < en) {
+                        const uint2 pr = __ldg(pairs + m);
+                        atomicAdd(e + ((int)pr.x + off), -du * half_lo(pr.y));
+                        if (pr.y >> 16) atomicAdd(e + ((int)pr.x + off + 1), -du * half_hi(pr.y));
+                    }
+                }
+            }
+            n_ent += (unsigned long long)n_entries;
+            ++n_upd;
+        }
+        __syncthreads();  // s_item / s_red reused by the next item
+    }
+    flush_counts(stats, n_upd, n_ent, tid);
+}
+
 // Lockstep stacks: one CTA of kStack warps per slice stack (the same-parity
 // slices of one physical cell, consecutive in the visiting order; the stack
 // table lists where each starts). Members start at the stack's common data
@@ -1256,7 +1406,7 @@ struct GraphKey {
     const float* e;
     const float* x;
     uint64_t in_flight;
-    int stage, wpv, epl, h;
+    int stage, pairs, wpv, epl, h;
 };
 
 
@@ -1355,6 +1505,10 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     unsigned long long* stats = ctx->d_queue + 2;
     const int wsel = o.weights ? o.weights : CTBB_SSM_FP32;
     const bool h = wsel == CTBB_SSM_FP16;
+    // Entry pairs for the CTA-per-update kernels with FP16 weights (built
+    // here, outside any stream capture, on first use).
+    if (h && wpv > 1 && o.entry_pairs == 0) CTBB_TRY(ssm_build_pairs(const_cast<ctbb_ssm*>(ssm)));
+    const bool pairs = h && wpv > 1 && o.entry_pairs == 0 && ssm->d_pairs;
     const int64_t* cp = ssm->d_colptr;
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
@@ -1423,6 +1577,16 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
                     icd_grouped_kernel<float, 8><<<blocks, 256, 0, s>>>(P, order, cp, vp, ix, ssm->d_w32, rc->d_start,
                                                                         rc->d_e32, rc->d_x32, ctx->d_queue, stats);
             }
+        } else if (pairs) {
+            const int blocks = (int)in_flight;
+            if (wpv == 8)
+                icd_cta_pairs_kernel<8, 16><<<blocks, 256, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                   ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                   rc->d_x32, ctx->d_queue, stats);
+            else
+                icd_cta_pairs_kernel<4, 16><<<blocks, 128, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                   ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                   rc->d_x32, ctx->d_queue, stats);
         } else {
             const int blocks = (int)in_flight;
             if (wpv == 8) {
@@ -1453,12 +1617,13 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     key.P = P;
     key.order = order;
     key.stacks = stacks;
-    key.w = h ? (const void*)ssm->d_w16 : (const void*)ssm->d_w32;
+    key.w = pairs ? (const void*)ssm->d_pairs : h ? (const void*)ssm->d_w16 : (const void*)ssm->d_w32;
     key.idx = ix;
     key.e = rc->d_e32;
     key.x = rc->d_x32;
     key.in_flight = in_flight;
     key.stage = stage;
+    key.pairs = pairs ? 1 : 0;
     key.wpv = wpv;
     key.epl = epl;
     key.h = h;

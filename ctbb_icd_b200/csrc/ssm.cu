@@ -275,8 +275,55 @@ __global__ void f32_to_f16_kernel(const float* __restrict__ in, __half* __restri
         out[i] = __float2half_rn(in[i]);
 }
 
+// Entry pairs: the modified-Joseph z interpolation gives every (view,
+// channel) of a column two adjacent detector rows, so its entries come in
+// runs of two consecutive sinogram indices. A pair {q, w0 | w1 << 16} holds
+// both FP16 weights of a run in 8 bytes (4 per entry instead of 6); a lone
+// entry has w1 = 0. One thread per (column, view) cell: pair count, then
+// (after the same per-column / per-matrix scans as the entries) the fill.
+template <bool FILL>
+__global__ void __launch_bounds__(256) ssm_pairs_kernel(uint64_t ncol, int nvsm, const int64_t* __restrict__ colptr,
+                                                        const uint32_t* __restrict__ vptr,
+                                                        const int32_t* __restrict__ idx,
+                                                        const __half* __restrict__ w16, uint16_t* __restrict__ cnt,
+                                                        const int64_t* __restrict__ pcolptr,
+                                                        const uint32_t* __restrict__ pvptr, uint2* __restrict__ pairs) {
+    const uint64_t ncell = ncol * (uint64_t)nvsm;
+    for (uint64_t t = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; t < ncell; t += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t col = t / (uint64_t)nvsm;
+        const int v = (int)(t % (uint64_t)nvsm);
+        const uint32_t* vp = vptr + col * (uint64_t)(nvsm + 1);
+        const int64_t b = colptr[col] + vp[v], en = colptr[col] + vp[v + 1];
+        uint2* out = nullptr;
+        if (FILL) out = pairs + pcolptr[col] + pvptr[col * (uint64_t)(nvsm + 1) + v];
+        int n = 0;
+        for (int64_t m = b; m < en;) {
+            const bool two = m + 1 < en && idx[m + 1] == idx[m] + 1;
+            if (FILL) {
+                const uint32_t lo = __half_as_ushort(w16[m]);
+                const uint32_t hi = two ? __half_as_ushort(w16[m + 1]) : 0u;
+                out[n] = make_uint2((uint32_t)idx[m], lo | (hi << 16));
+            }
+            ++n;
+            m += two ? 2 : 1;
+        }
+        if (!FILL) cnt[t] = (uint16_t)n;
+    }
+}
+
+void free_pairs(ctbb_ssm* s) {
+    cudaFree(s->d_pcolptr);
+    cudaFree(s->d_pvptr);
+    cudaFree(s->d_pairs);
+    s->d_pcolptr = nullptr;
+    s->d_pvptr = nullptr;
+    s->d_pairs = nullptr;
+    s->npairs = 0;
+}
+
 void free_ssm(ctbb_ssm* s) {
     if (!s) return;
+    free_pairs(s);
     cudaFree(s->d_colptr);
     cudaFree(s->d_vptr);
     cudaFree(s->d_idx);
@@ -392,6 +439,62 @@ ctbb_status ssm_validate_geometry(const ctbb_geom_c& g) {
     if (g.voxel_size_x <= 0 || g.voxel_size_y <= 0 || g.voxel_size_z <= 0)
         return fail(CTBB_ERR_INVALID_ARG, "non-positive voxel size");
     return CTBB_OK;
+}
+
+// Build (once) the pair form of an FP16 matrix (ssm_pairs_kernel).
+ctbb_status ssm_build_pairs(ctbb_ssm* s) {
+    if (s->d_pairs || s->pairs_checked) return CTBB_OK;
+    if (!s->d_w16) return fail(CTBB_ERR_INVALID_ARG, "entry pairs need the matrix's FP16 weights");
+    ctbb_ctx* ctx = s->ctx;
+    cudaStream_t st = ctx->stream;
+    const uint64_t ncell = s->ncol * s->nvsm;
+    uint16_t* d_cnt = nullptr;
+    uint64_t* d_tot = nullptr;
+    unsigned long long* d_max = nullptr;
+    struct Tmp {
+        void* p[3] = {nullptr, nullptr, nullptr};
+        ~Tmp() {
+            for (void* q : p) cudaFree(q);
+        }
+    } tmp;
+    ctbb_status rc = CTBB_OK;
+    auto run = [&]() -> ctbb_status {
+        CTBB_CUDA(cudaMalloc(&d_cnt, std::max<uint64_t>(1, ncell) * sizeof(uint16_t)));
+        tmp.p[0] = d_cnt;
+        CTBB_CUDA(cudaMalloc(&d_tot, std::max<uint64_t>(1, s->ncol) * sizeof(uint64_t)));
+        tmp.p[1] = d_tot;
+        CTBB_CUDA(cudaMalloc(&d_max, sizeof(unsigned long long)));
+        tmp.p[2] = d_max;
+        CTBB_CUDA(cudaMemsetAsync(d_max, 0, sizeof(unsigned long long), st));
+        CTBB_CUDA(cudaMalloc(&s->d_pcolptr, (s->ncol + 1) * sizeof(int64_t)));
+        CTBB_CUDA(cudaMalloc(&s->d_pvptr, s->ncol * (s->nvsm + 1) * sizeof(uint32_t)));
+        const int grid = grid_for(ctx, ncell, 256);
+        ssm_pairs_kernel<false><<<grid, 256, 0, st>>>(s->ncol, (int)s->nvsm, s->d_colptr, s->d_vptr, s->d_idx,
+                                                      s->d_w16, d_cnt, nullptr, nullptr, nullptr);
+        CTBB_CUDA(cudaGetLastError());
+        ssm_column_scan_kernel<<<(int)std::min<uint64_t>(s->ncol, (uint64_t)ctx->sm_count * 32), 256, 0, st>>>(
+            d_cnt, (int)s->nvsm, s->ncol, s->d_pvptr, d_tot);
+        CTBB_CUDA(cudaGetLastError());
+        ssm_colptr_kernel<<<1, 1024, 0, st>>>(d_tot, s->ncol, s->d_pcolptr, d_max);
+        CTBB_CUDA(cudaGetLastError());
+        int64_t np = 0;
+        CTBB_CUDA(cudaMemcpyAsync(&np, s->d_pcolptr + s->ncol, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+        CTBB_CUDA(cudaStreamSynchronize(st));
+        s->npairs = (uint64_t)np;
+        CTBB_CUDA(cudaMalloc(&s->d_pairs, std::max<uint64_t>(1, s->npairs) * sizeof(uint2)));
+        ssm_pairs_kernel<true><<<grid, 256, 0, st>>>(s->ncol, (int)s->nvsm, s->d_colptr, s->d_vptr, s->d_idx,
+                                                     s->d_w16, nullptr, s->d_pcolptr, s->d_pvptr, s->d_pairs);
+        CTBB_CUDA(cudaGetLastError());
+        CTBB_CUDA(cudaStreamSynchronize(st));
+        return CTBB_OK;
+    };
+    rc = run();
+    s->pairs_checked = true;
+    // Pairs pay only where most runs are two rows long (8 bytes per pair
+    // against 6 per entry): with fewer than 4 entries per 3 pairs (the z
+    // flying focal spot splits the runs) the single entries are kept.
+    if (rc != CTBB_OK || 4 * s->npairs > 3 * s->nnz) free_pairs(s);
+    return rc;
 }
 
 }  // namespace ctbb
@@ -532,6 +635,7 @@ extern "C" ctbb_status ctbb_gpu_ssm_info(const ctbb_ssm* s, ctbb_ssm_info* info)
     info->weights = s->weights;
     info->ffs = s->ffs;
     info->build_ms = s->build_ms;
+    info->n_pairs = s->npairs;
     return CTBB_OK;
 }
 

@@ -52,7 +52,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     // staged kernel with 4 or 8 updates per SM; one warp per voxel streaming the column twice at
     // 1/4 .. 2 times the coupling-bound default; 8 or 16 entries per lane in
     // flight, the default tile edge for that concurrency (and half of it);
-    // 4 warps per voxel with four updates per SM. Launches cap the updates in
+    // 4 or 8 warps per voxel with four or eight updates per SM. Launches cap the updates in
     // flight at the visiting order's bound, so candidates that collapse onto
     // the same effective shape run once.
     const int w0 = default_warps_in_flight(rc);
@@ -79,7 +79,11 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             cands.push_back({1, w, epl, 0, 0});
             if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1, 0});
         }
+    // Several warps per update (the column's entries, or entry pairs with
+    // FP16 weights, kept in registers): four or eight updates per SM.
     cands.push_back({4, 4 * sms * 4, 8, 0, 0});
+    cands.push_back({4, 8 * sms * 4, 8, 0, 0});
+    cands.push_back({8, 4 * sms * 8, 8, 0, 0});
     struct Trial {
         int wpv, w, epl, t, stage;
         double ms, cost, score;

@@ -230,6 +230,8 @@ typedef struct ctbb_ssm_info {
     int32_t weights;        /* CTBB_SSM_* held                             */
     int32_t ffs;            /* 1 if built with a flying focal spot (in-plane and/or z) */
     double build_ms;        /* device time of the last build               */
+    uint64_t n_pairs;       /* entry pairs (0 until a grouped iteration with
+                               entry_pairs has built them)                 */
 } ctbb_ssm_info;
 
 /*
@@ -298,6 +300,13 @@ typedef struct ctbb_icd_opts {
                                  warps sweep the stack's data views in lockstep,
                                  so the sinogram sectors they share are fetched
                                  from HBM once                                     */
+    int32_t entry_pairs;      /* grouped, FP16 weights, 4 or 8 warps per voxel: 0
+                                 reads the matrix as entry pairs ({sinogram index,
+                                 two FP16 weights} for the two detector rows of a
+                                 (view, channel): 4 bytes per entry, built once per
+                                 matrix on first use and kept where pairs hold
+                                 4/3 entries or more on average); -1 reads single
+                                 entries (4-byte index + 2-byte weight)           */
 } ctbb_icd_opts;
 
 /*
@@ -451,12 +460,13 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
  * schedule) and keeps the one with the
  * largest decrease of the FP64 cost per millisecond of device time. The
  * iterate and e are restored afterwards; *best = *base with those fields
- * set. Candidates: the lockstep stack kernel (stage_column 3) with 8 or 16
+ * set. Candidates: the lockstep stack kernel (stage_column 3) with 8
  * entries per lane; the shared-memory staged kernel (stage_column 1, 2);
  * one warp per voxel at 1/4, 1/2, 1 and 2 times the
  * coupling-bound default of warps in flight, with 8 or 16 entries per lane
  * in flight and the default tile edge for that concurrency (half of it too
- * at the default); 4 warps per voxel with four updates per SM.
+ * at the default); 4 warps per voxel with four or eight updates per SM and
+ * 8 warps per voxel with four (these read entry pairs with FP16 weights).
  * Every launch keeps at most one cell rank of the visiting order (about
  * n / T^2 updates for tile edge T) in flight, so no two in-plane neighbours
  * of a slice are ever updated together; trials report the effective warps

@@ -197,10 +197,13 @@ def converged_cfg1_small(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights,wpv,stage", [(C.SSM_FP32, 1, 0), (C.SSM_FP16, 1, 0), (C.SSM_FP32, 8, 0),
-                                               (C.SSM_FP16, 4, 0), (C.SSM_FP16, 1, 1), (C.SSM_FP32, 1, 2),
-                                               (C.SSM_FP16, 1, 3), (C.SSM_FP32, 1, 3)])
-def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage):
+@pytest.mark.parametrize("weights,wpv,stage,pairs", [
+    (C.SSM_FP32, 1, 0, 0), (C.SSM_FP16, 1, 0, 0), (C.SSM_FP32, 8, 0, 0), (C.SSM_FP16, 4, 0, 0),
+    (C.SSM_FP16, 8, 0, 0), (C.SSM_FP16, 4, 0, -1), (C.SSM_FP16, 1, 1, 0), (C.SSM_FP32, 1, 2, 0),
+    (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0)])
+def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage, pairs):
+    """FP16 with 4 or 8 warps per update reads the matrix as entry pairs
+    (pairs 0) or as single entries (pairs -1)."""
     rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
     rc = C.Recon(rp, data.slice_indices, ctx)
     rc.set_raw(data.raw)
@@ -208,7 +211,7 @@ def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, 
     costs = []
     for _ in range(6):
         rc.iterate(ssm, 5, C.icd_opts(mode=C.ICD_GROUPED, weights=weights, refresh_every=5, warps_per_voxel=wpv,
-                                      stage_column=stage))
+                                      stage_column=stage, entry_pairs=pairs))
         rc.refresh_residual(ssm)
         costs.append(rc.cost())
     x = rc.volume_f64()
@@ -216,6 +219,29 @@ def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, 
     assert all(b <= a * (1 + 1e-9) for a, b in zip(costs, costs[1:])), costs
     assert rmse_hu <= 0.5, rmse_hu
     assert abs(costs[-1] - cost_ref) <= 1e-6 * abs(cost_ref), (costs[-1], cost_ref)
+
+
+@pytest.mark.parametrize("wpv", [4, 8])
+def test_entry_pairs_match_single_entries(ctx, converged_cfg1_small, wpv):
+    """One update in flight (the visiting order run one voxel at a time):
+    the pair form of the FP16 matrix gives the same iterates as its single
+    entries, up to the order of the FP32 partial sums (each thread sums a
+    different share of the column)."""
+    rp, data, ssm, _, _ = converged_cfg1_small
+    out = {}
+    for pairs in (0, -1):
+        rc = C.Recon(rp, data.slice_indices, ctx)
+        rc.set_raw(data.raw)
+        rc.set_volume(ssm, None)
+        rc.iterate(ssm, 2, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP16, warps_per_voxel=wpv,
+                                      warps_in_flight=wpv, entry_pairs=pairs))
+        out[pairs] = rc.volume_f64()
+        rc.free()
+    assert ssm.info().n_pairs > 0
+    # every run of the z interpolation is two rows: about half as many pairs as entries
+    assert abs(ssm.info().n_pairs - ssm.info().nnz / 2) <= 0.01 * ssm.info().nnz
+    a, b = out[0], out[-1]
+    assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
 def test_batch_of_uneven_scans_converges(ctx, converged_cfg1_small, tmp_path):
