@@ -210,8 +210,8 @@ def run_ours(args, rank, world, dist):
     # The matrix in the form the kernel reads: entry pairs (8 B per pair of
     # rows) when the iteration used them, else index + weight per entry.
     n_pairs = int(ssm.info().n_pairs)
-    uses_pairs = (n_pairs > 0 and weights_fmt == C.SSM_FP16 and opts.warps_per_voxel > 1
-                  and opts.entry_pairs == 0)
+    uses_pairs = (n_pairs > 0 and weights_fmt == C.SSM_FP16 and opts.entry_pairs == 0
+                  and (opts.warps_per_voxel > 1 or opts.stage_column == 0))
     ssm_read = 8.0 * n_pairs if uses_pairs else (4 + w_bytes) * float(info.nnz)
     b_iter = 4.0 * gathered + 4.0 * scattered + ssm_read + 8.0 * nvox
 
@@ -231,7 +231,8 @@ def run_ours(args, rank, world, dist):
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
         kernel = ("icd_lockstep_kernel" if opts.stage_column == 3 else
-                  "icd_staged_kernel" if opts.stage_column else "icd_grouped_kernel") \
+                  "icd_staged_kernel" if opts.stage_column else
+                  "icd_grouped_pairs_kernel" if uses_pairs else "icd_grouped_kernel") \
             if opts.warps_per_voxel <= 1 else ("icd_cta_pairs_kernel" if uses_pairs else "icd_cta_kernel")
         traffic = read_traffic(kernel)
         out = {

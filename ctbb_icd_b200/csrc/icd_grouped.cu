@@ -144,6 +144,10 @@ __device__ __forceinline__ void load_chunk(const int32_t* __restrict__ idx, cons
     }
 }
 
+// The two FP16 weights of an entry pair ({q, w0 | w1 << 16}).
+__device__ __forceinline__ float half_lo(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+__device__ __forceinline__ float half_hi(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
+
 constexpr int kU = 8;       // entries per lane in flight per chunk (default)
 constexpr int kStack = 16;  // same-parity slices that sweep the sinogram together
 
@@ -474,6 +478,134 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
     flush_counts(stats, n_upd, n_ent, lane);
 }
 
+// One warp per update over the matrix's entry pairs (the streamed kernel's
+// order, stack start view and round trips; the pair form halves the matrix
+// loads and reads 4 bytes per entry instead of 6). Lane l takes pairs
+// m, m + 32, ... of a chunk of 32 x U pairs; each pair is one 8-byte load and
+// one or two e gathers.
+template <int U>
+__device__ __forceinline__ void load_pairs(const uint2* __restrict__ pairs, int64_t m, int64_t en, int off,
+                                           uint64_t pol, int* q, uint32_t* wp) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int64_t mu = m + 32 * u;
+        if (mu < en) {
+            uint32_t a, bb;
+            asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                         : "=r"(a), "=r"(bb)
+                         : "l"(pairs + mu), "l"(pol));
+            q[u] = (int)a + off;
+            wp[u] = bb;
+        } else {
+            q[u] = -1;
+            wp[u] = 0u;
+        }
+    }
+}
+
+template <int U>
+__device__ __forceinline__ void gather_pairs(const uint2* __restrict__ pairs, const float* e, int64_t b, int64_t en,
+                                             int off, int lane, uint64_t pol, float& acc_b, float& acc_a) {
+    if (b >= en) return;
+    int qa[U];
+    uint32_t wa[U];
+    load_pairs<U>(pairs, b + lane, en, off, pol, qa, wa);
+    for (int64_t base = b; base < en; base += 32 * U) {
+        float e0[U], e1[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            e0[u] = qa[u] >= 0 ? __ldcg(e + qa[u]) : 0.f;
+            e1[u] = (qa[u] >= 0 && (wa[u] >> 16)) ? __ldcg(e + qa[u] + 1) : 0.f;
+        }
+        int qb[U];
+        uint32_t wb[U];
+        load_pairs<U>(pairs, base + 32 * U + lane, en, off, pol, qb, wb);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const float w0 = half_lo(wa[u]), w1 = half_hi(wa[u]);
+            acc_b = fmaf(w0, e0[u], acc_b);
+            acc_b = fmaf(w1, e1[u], acc_b);
+            acc_a = fmaf(w0, w0, acc_a);
+            acc_a = fmaf(w1, w1, acc_a);
+            qa[u] = qb[u];
+            wa[u] = wb[u];
+        }
+    }
+}
+
+template <int U>
+__device__ __forceinline__ void scatter_pairs(const uint2* __restrict__ pairs, float* e, int64_t b, int64_t en,
+                                              int off, int lane, uint64_t pol, float du) {
+    if (b >= en) return;
+    const int64_t nchunk = (en - b + 32 * U - 1) / (32 * U);
+    for (int64_t c = nchunk - 1; c >= 0; --c) {
+        int qs[U];
+        uint32_t ws[U];
+        load_pairs<U>(pairs, b + c * (32 * U) + lane, en, off, pol, qs, ws);
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            if (qs[u] >= 0) {
+                atomicAdd(e + qs[u], -du * half_lo(ws[u]));
+                if (ws[u] >> 16) atomicAdd(e + qs[u] + 1, -du * half_hi(ws[u]));
+            }
+    }
+}
+
+template <int U>
+__global__ void __launch_bounds__(256) icd_grouped_pairs_kernel(
+    GParams P, const uint32_t* __restrict__ order, const int64_t* __restrict__ pcolptr,
+    const uint32_t* __restrict__ pvptr, const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
+    const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue, unsigned long long* stats) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    unsigned long long n_ent = 0, n_upd = 0;
+    for (;;) {
+        unsigned long long item = 0;
+        if (lane == 0) item = atomicAdd(queue, 1ull);
+        item = __shfl_sync(0xffffffffu, item, 0);
+        if (item >= P.n_items) break;
+        const uint32_t packed = __ldg(order + item);
+        const uint64_t col = packed / (uint32_t)P.nz;
+        const int k = (int)(packed % (uint32_t)P.nz);
+        const int64_t q = (int64_t)col + (int64_t)ncol * k;
+        const int s = start[k];
+        const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+        int64_t b = 0, en = 0, mid = 0, n_entries = 0;
+        if (v1 > v0) {
+            const int64_t cb = pcolptr[col];
+            const uint32_t* vp = pvptr + col * P.nvsm1;
+            b = cb + vp[v0];
+            en = cb + vp[v1];
+            // Same common start view for the members of a slice stack as
+            // process_item.
+            const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1),
+                               ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
+            mid = cb + vp[min(max(start[kl] - s, v0), v1)];
+            n_entries = (int64_t)vptr[col * P.nvsm1 + v1] - (int64_t)vptr[col * P.nvsm1 + v0];
+        }
+        const int off = s * P.nch * P.nr;
+        float acc_b = 0.f, acc_a = 0.f;
+        const uint64_t keep = l2_keep();
+        gather_pairs<U>(pairs, e, mid, en, off, lane, keep, acc_b, acc_a);
+        gather_pairs<U>(pairs, e, b, mid, off, lane, keep, acc_b, acc_a);
+        const double beta = (double)warp_sum(acc_b);
+        const double alpha = (double)warp_sum(acc_a);
+        const double xq = (double)__ldcg(x + q);
+        double upd = penalty_step(P, x, q, xq, alpha, beta, lane) * P.relax;
+        if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+        if (lane == 0) x[q] = (float)(xq + upd);
+        const float du = (float)upd;
+        if (du != 0.f) {
+            const uint64_t drop = l2_drop();
+            scatter_pairs<U>(pairs, e, b, mid, off, lane, drop, du);
+            scatter_pairs<U>(pairs, e, mid, en, off, lane, drop, du);
+            n_ent += (unsigned long long)n_entries;
+            ++n_upd;
+        }
+    }
+    flush_counts(stats, n_upd, n_ent, lane);
+}
+
 // Entries p0, p0+32, ..., p0+32(U-1) of an item's entry sequence: positions
 // [0, n1) are matrix entries [mid, en) (the stack's common start view to the
 // end of the slice's window), positions [n1, n) entries [b, mid); hi = mid,
@@ -502,8 +634,6 @@ __device__ __forceinline__ void load_seq(const int32_t* __restrict__ idx, const 
 // read from HBM once; longer columns re-read their tail. Same update as
 // icd_cta_kernel; the entry counts (for the statistics) come from the entry
 // offsets.
-__device__ __forceinline__ float half_lo(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
-__device__ __forceinline__ float half_hi(uint32_t w) { return __half2float(__ushort_as_half((unsigned short)(w >> 16))); }
 
 template <int WPV, int R>
 __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
@@ -1507,8 +1637,9 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const bool h = wsel == CTBB_SSM_FP16;
     // Entry pairs for the CTA-per-update kernels with FP16 weights (built
     // here, outside any stream capture, on first use).
-    if (h && wpv > 1 && o.entry_pairs == 0) CTBB_TRY(ssm_build_pairs(const_cast<ctbb_ssm*>(ssm)));
-    const bool pairs = h && wpv > 1 && o.entry_pairs == 0 && ssm->d_pairs;
+    const bool want_pairs = h && o.entry_pairs == 0 && (wpv > 1 || stage == 0);
+    if (want_pairs) CTBB_TRY(ssm_build_pairs(const_cast<ctbb_ssm*>(ssm)));
+    const bool pairs = want_pairs && ssm->d_pairs;
     const int64_t* cp = ssm->d_colptr;
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
@@ -1560,7 +1691,17 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
                 P, order, ssm, ssm->d_w32, rc, in_flight, stats, s, prepare);
         }
         if (prepare) return CTBB_OK;
-        if (wpv == 1) {
+        if (wpv == 1 && pairs) {
+            const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
+            if (epl == 16)
+                icd_grouped_pairs_kernel<16><<<blocks, 256, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                    ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                    rc->d_x32, ctx->d_queue, stats);
+            else
+                icd_grouped_pairs_kernel<8><<<blocks, 256, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                   ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                   rc->d_x32, ctx->d_queue, stats);
+        } else if (wpv == 1) {
             const int blocks = (int)std::max<uint64_t>(1, (in_flight + 7) / 8);
             if (epl == 16) {
                 if (h)

@@ -300,7 +300,9 @@ typedef struct ctbb_icd_opts {
                                  warps sweep the stack's data views in lockstep,
                                  so the sinogram sectors they share are fetched
                                  from HBM once                                     */
-    int32_t entry_pairs;      /* grouped, FP16 weights, 4 or 8 warps per voxel: 0
+    int32_t entry_pairs;      /* grouped, FP16 weights, one warp per voxel (streamed,
+                                 stage_column 0; entries_per_lane then counts pairs)
+                                 or 4 or 8 warps per voxel: 0
                                  reads the matrix as entry pairs ({sinogram index,
                                  two FP16 weights} for the two detector rows of a
                                  (view, channel): 4 bytes per entry, built once per

@@ -198,12 +198,12 @@ def converged_cfg1_small(ctx, tmp_path_factory):
 
 
 @pytest.mark.parametrize("weights,wpv,stage,pairs", [
-    (C.SSM_FP32, 1, 0, 0), (C.SSM_FP16, 1, 0, 0), (C.SSM_FP32, 8, 0, 0), (C.SSM_FP16, 4, 0, 0),
+    (C.SSM_FP32, 1, 0, 0), (C.SSM_FP16, 1, 0, 0), (C.SSM_FP16, 1, 0, -1), (C.SSM_FP32, 8, 0, 0), (C.SSM_FP16, 4, 0, 0),
     (C.SSM_FP16, 8, 0, 0), (C.SSM_FP16, 4, 0, -1), (C.SSM_FP16, 1, 1, 0), (C.SSM_FP32, 1, 2, 0),
     (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0)])
 def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage, pairs):
-    """FP16 with 4 or 8 warps per update reads the matrix as entry pairs
-    (pairs 0) or as single entries (pairs -1)."""
+    """FP16 with the streamed (one warp) or 4/8-warp kernels reads the
+    matrix as entry pairs (pairs 0) or as single entries (pairs -1)."""
     rp, data, ssm, x_ref, cost_ref = converged_cfg1_small
     rc = C.Recon(rp, data.slice_indices, ctx)
     rc.set_raw(data.raw)
