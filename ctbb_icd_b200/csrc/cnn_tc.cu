@@ -8,21 +8,25 @@
 // Shared memory (no swizzle, K-major canonical layout: rows of 16 bytes =
 // 8 channels, row r of a region at byte 16 r):
 //   weights  27 taps x 4 channel chunks x 32 rows (co)          54 KB, once
-//   halo x2  9 input lines (dz, dy in -1..1) x 4 chunks x 130 rows
-//            (x0-1 .. x0+128), one TMA box per (line, chunk), each chunk
-//            region padded to 2176 bytes (128-byte aligned)      77 KB each
+//   halo x2  9 input lines (dz, dy in -1..1), each one TMA box of
+//            4 chunk regions x 130 rows (x0-1 .. x0+128): the tensor map
+//            orders its dimensions (8 channels, x, chunk, y, z), so the box
+//            lands chunk-major, 2080 bytes per chunk, 8320 per line
+//            (a multiple of 128: every box starts 128-byte aligned)  73 KB each
 // Tap (dx, dy, dz) reads line (dz, dy) starting at row 1 + dx, so the 27 A
 // operands are descriptors into the same halo (start address shifted by
 // 16 bytes per voxel); the borders come from the TMA's zero fill.
 //
-// One elected thread issues the TMA loads and the 54 MMAs (27 taps x 2
-// K-halves of 16 channels) and commits them to an mbarrier; all four warps
-// then read their 32 TMEM lanes (tcgen05.ld 32x32b) and apply the epilogue
-// (+ bias, + residual, zero where mask <= 0, relu) as conv_mid_kernel does.
-// Halo and accumulator are double-buffered: the loads of tile i+1 run while
-// tile i is multiplied and written out. Every wait on an mbarrier is bounded;
-// on expiry the kernel records a code in the device error flag and returns
-// after releasing its tensor memory.
+// One elected thread issues the TMA loads (9 boxes per tile) and the 54
+// MMAs (27 taps x 2 K-halves of 16 channels) and commits them to an
+// mbarrier; all four warps then read their 32 TMEM lanes (tcgen05.ld
+// 32x32b) and apply the epilogue (+ bias, + residual, zero where mask <= 0,
+// relu) as conv_mid_kernel does. Halo and accumulator are double-buffered
+// and the schedule is software-pipelined: the MMAs of tile i+1 are issued
+// before the epilogue of tile i, and the halo of tile i+2 is loaded as soon
+// as the MMAs of tile i have read theirs. Every wait on an mbarrier is
+// bounded; on expiry the kernel records a code in the device error flag and
+// returns after its copies have landed and its tensor memory is released.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <string.h>
@@ -38,13 +42,9 @@ constexpr int kC = 32;
 constexpr int kTaps = 27;
 constexpr int kM = 128;                         // output voxels per tile
 constexpr int kLine = kM + 2;                   // input voxels per halo line
-// One 8-channel chunk of a line: kLine rows of 16 bytes (2080), padded to a
-// multiple of 128 bytes because a tiled TMA copy must land on a 128-byte
-// aligned shared-memory address.
-constexpr int kChunkBytes = ((kLine * 16 + 127) / 128) * 128;  // 2176
-constexpr int kBoxBytes = kLine * 16;           // 2080 bytes land per TMA box
-constexpr int kLineBytes = 4 * kChunkBytes;     // 8704
-constexpr int kHaloBytes = 9 * kLineBytes;      // 78336
+constexpr int kChunkBytes = kLine * 16;         // 2080: one 8-channel chunk of a line
+constexpr int kLineBytes = 4 * kChunkBytes;     // 8320: one TMA box
+constexpr int kHaloBytes = 9 * kLineBytes;      // 74880
 constexpr int kTapWBytes = 4 * kC * 16;         // 2048
 constexpr int kWBytes = kTaps * kTapWBytes;     // 55296
 constexpr int kOffHalo0 = kWBytes;
@@ -54,8 +54,9 @@ constexpr int kOffTmem = kOffBar + 4 * 8;
 constexpr int kSmemBytes = kOffTmem + 16;
 constexpr int kThreads = 128;
 constexpr int kTmemCols = 64;                    // two 32-column accumulators
-static_assert(kChunkBytes % 128 == 0 && kLineBytes % 128 == 0 && kHaloBytes % 128 == 0 && kWBytes % 128 == 0,
-              "TMA destinations must stay 128-byte aligned");
+static_assert(kLineBytes % 128 == 0 && kHaloBytes % 128 == 0 && kWBytes % 128 == 0,
+              "TMA destinations (one per halo line) must stay 128-byte aligned");
+static_assert(kChunkBytes % 16 == 0, "matrix descriptor offsets are in 16-byte units");
 static_assert(kSmemBytes <= 227 * 1024, "shared memory per CTA");
 
 // Instruction descriptor of tcgen05.mma kind::f16: D FP32, A and B BF16,
@@ -150,20 +151,36 @@ __device__ __forceinline__ void tile_coords(const TcDims& d, uint64_t t, int& x0
     z = (int)(r / d.ny);
 }
 
-// The 36 TMA boxes of one tile's halo: line (dz, dy), chunk c -> rows
-// x0-1 .. x0+128 of input line (y+dy, z+dz), 16 bytes (8 channels) each.
+// The 9 TMA boxes of one tile's halo: line (dz, dy) -> 4 chunk regions of
+// rows x0-1 .. x0+128 of input line (y+dy, z+dz), 16 bytes (8 channels) each.
 __device__ __forceinline__ void issue_halo(const CUtensorMap* map, uint32_t halo, uint32_t bar, const TcDims& d,
                                            uint64_t t) {
     int x0, y, z;
     tile_coords(d, t, x0, y, z);
-    mbar_expect_tx(bar, (uint32_t)(9 * 4 * kBoxBytes));  // bytes delivered, not the padded stride
+    mbar_expect_tx(bar, (uint32_t)kHaloBytes);
 #pragma unroll 1
     for (int line = 0; line < 9; ++line) {
         const int dz = line / 3 - 1, dy = line % 3 - 1;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-            tma_load_5d(halo + (uint32_t)(line * kLineBytes + c * kChunkBytes), map, bar, 0, c, x0 - 1, y + dy, z + dz);
+        tma_load_5d(halo + (uint32_t)(line * kLineBytes), map, bar, 0, x0 - 1, 0, y + dy, z + dz);
     }
+}
+
+// The 54 MMAs of one tile (27 taps x 2 K-halves) into a TMEM accumulator,
+// committed to an mbarrier (one thread).
+__device__ __forceinline__ void issue_mmas(uint32_t d_tmem, uint32_t halo, uint32_t s_w, uint32_t bar) {
+#pragma unroll 1
+    for (int tap = 0; tap < kTaps; ++tap) {
+        const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;  // offsets + 1
+        const uint32_t a0 = halo + (uint32_t)((dz * 3 + dy) * kLineBytes + dx * 16);
+        const uint32_t w0 = s_w + (uint32_t)(tap * kTapWBytes);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const uint64_t ad = smem_desc(a0 + (uint32_t)(2 * h * kChunkBytes), kChunkBytes, 128);
+            const uint64_t bd = smem_desc(w0 + (uint32_t)(2 * h * 512), 512, 128);
+            mma_bf16(d_tmem, ad, bd, (tap | h) ? 1u : 0u);
+        }
+    }
+    mma_commit(bar);
 }
 
 __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_constant__ CUtensorMap in_map,
@@ -179,7 +196,6 @@ __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_c
     auto bar_load = [&](int b) { return s_base + (uint32_t)(kOffBar + 8 * b); };
     auto bar_mma = [&](int b) { return s_base + (uint32_t)(kOffBar + 16 + 8 * b); };
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(smem + kOffTmem);
-    __shared__ int s_abort;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
     // Weights [tap][co][ci] -> chunk-major K-major rows: tap t, chunk c,
@@ -190,7 +206,6 @@ __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_c
         *reinterpret_cast<uint4*>(smem + t * kTapWBytes + c * 512 + co * 16) = v;
     }
     if (tid == 0) {
-        s_abort = 0;
         for (int i = 0; i < 4; ++i) mbar_init(s_base + kOffBar + 8 * i, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
@@ -218,47 +233,53 @@ __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_c
         return;
     }
 
-    // Phase parity of each barrier (bit b), advanced only after a completed wait.
+    // Phase parity of each barrier (bit b), advanced only after a completed
+    // wait. A wait that runs out in any thread ends the loop in every thread
+    // (__syncthreads_or), so all threads take the same barriers.
     uint32_t ph_load = 0, ph_mma = 0;
-    const uint64_t first = blockIdx.x;
-    if (tid == 0 && first < d.n_tiles) issue_halo(&in_map, s_halo(0), bar_load(0), d, first);
-    int i = 0;
-    for (uint64_t t = first; t < d.n_tiles; t += gridDim.x, ++i) {
-        const int b = i & 1;
-        if (mbar_wait(bar_load(b), (ph_load >> b) & 1))
-            ph_load ^= 1u << b;
-        else
-            s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
-        fence_after();
+    bool aborted = false;
+    const uint64_t first = blockIdx.x, step = gridDim.x;
+    // Prologue: halos of the first two tiles, MMAs of the first.
+    if (first < d.n_tiles) {
         if (tid == 0) {
-            const uint32_t d_tmem = tmem + (uint32_t)(b * kC);
-#pragma unroll 1
-            for (int tap = 0; tap < kTaps; ++tap) {
-                const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;  // offsets + 1
-                const uint32_t a0 = s_halo(b) + (uint32_t)((dz * 3 + dy) * kLineBytes + dx * 16);
-                const uint32_t w0 = s_w + (uint32_t)(tap * kTapWBytes);
-#pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint64_t ad = smem_desc(a0 + (uint32_t)(2 * h * kChunkBytes), kChunkBytes, 128);
-                    const uint64_t bd = smem_desc(w0 + (uint32_t)(2 * h * 512), 512, 128);
-                    mma_bf16(d_tmem, ad, bd, (tap | h) ? 1u : 0u);
-                }
-            }
-            mma_commit(bar_mma(b));
-            // The other halo buffer was last read by the MMAs of tile i-1,
-            // which completed before that tile's epilogue.
-            const uint64_t next = t + gridDim.x;
-            if (next < d.n_tiles) issue_halo(&in_map, s_halo(b ^ 1), bar_load(b ^ 1), d, next);
+            issue_halo(&in_map, s_halo(0), bar_load(0), d, first);
+            if (first + step < d.n_tiles) issue_halo(&in_map, s_halo(1), bar_load(1), d, first + step);
         }
-        if (mbar_wait(bar_mma(b), (ph_mma >> b) & 1))
-            ph_mma ^= 1u << b;
-        else
-            s_abort = 1;
-        __syncthreads();
-        if (s_abort) break;
+        const bool ok = mbar_wait(bar_load(0), 0);
+        if (ok) ph_load ^= 1u;
+        aborted = __syncthreads_or(!ok) != 0;
+        if (!aborted) {
+            fence_after();
+            if (tid == 0) issue_mmas(tmem, s_halo(0), s_w, bar_mma(0));
+        }
+    }
+    int i = 0;
+    for (uint64_t t = first; t < d.n_tiles && !aborted; t += step, ++i) {
+        const int b = i & 1, nb = b ^ 1;
+        const uint64_t next = t + step;
+        // MMAs of tile i+1 into the other accumulator (free since tile i-1's
+        // epilogue), once its halo has landed.
+        if (next < d.n_tiles) {
+            const bool ok = mbar_wait(bar_load(nb), (ph_load >> nb) & 1);
+            if (ok) ph_load ^= 1u << nb;
+            if (__syncthreads_or(!ok)) {
+                aborted = true;
+                break;
+            }
+            fence_after();
+            if (tid == 0) issue_mmas(tmem + (uint32_t)(nb * kC), s_halo(nb), s_w, bar_mma(nb));
+        }
+        // Tile i's MMAs done: its halo buffer is free for tile i+2.
+        {
+            const bool ok = mbar_wait(bar_mma(b), (ph_mma >> b) & 1);
+            if (ok) ph_mma ^= 1u << b;
+            if (__syncthreads_or(!ok)) {
+                aborted = true;
+                break;
+            }
+        }
         fence_after();
+        if (tid == 0 && next + step < d.n_tiles) issue_halo(&in_map, s_halo(b), bar_load(b), d, next + step);
         // Epilogue: warp w holds voxels 32 w .. 32 w + 31 of the tile.
         float acc[kC];
         tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)(b * kC), acc);
@@ -296,7 +317,7 @@ __global__ void __launch_bounds__(kThreads, 1) conv_mid_tc_kernel(const __grid_c
         fence_before();
         __syncthreads();  // TMEM buffer b read before the MMAs of tile i+2 overwrite it
     }
-    if (s_abort) {
+    if (aborted) {
         if (tid == 0) atomicExch(err, 1);
         // Let any TMA or MMA still in flight land before the memory goes away.
         for (int k = 0; k < 2; ++k) {
@@ -345,10 +366,11 @@ ctbb_status conv_mid_tc(ctbb_ctx* ctx, int nx, int ny, int nz, const __nv_bfloat
         return fail(CTBB_ERR_INVALID_ARG, "convolution buffers must be 16-byte aligned");
     CUtensorMap map;
     memset(&map, 0, sizeof(map));
-    // (8 channels, 4 chunks, x, y, z); strides of dims 1..4 in bytes.
-    const cuuint64_t dims[5] = {8, 4, (cuuint64_t)nx, (cuuint64_t)ny, (cuuint64_t)nz};
-    const cuuint64_t strides[4] = {16, 64, (cuuint64_t)64 * nx, (cuuint64_t)64 * nx * ny};
-    const cuuint32_t box[5] = {8, 1, (cuuint32_t)kLine, 1, 1};
+    // (8 channels, x, 4 chunks, y, z); strides of dims 1..4 in bytes. The
+    // chunk dimension comes after x so that one box lands chunk-major.
+    const cuuint64_t dims[5] = {8, (cuuint64_t)nx, 4, (cuuint64_t)ny, (cuuint64_t)nz};
+    const cuuint64_t strides[4] = {64, 16, (cuuint64_t)64 * nx, (cuuint64_t)64 * nx * ny};
+    const cuuint32_t box[5] = {8, (cuuint32_t)kLine, 4, 1, 1};
     const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
     const CUresult r = enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)in, dims, strides, box, estr,
                            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
