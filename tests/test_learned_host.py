@@ -51,6 +51,8 @@ def test_committed_weights_and_protocol():
 
     assert d["params"].shape == (O.num_params(int(d["blocks"])),) and np.isfinite(d["params"]).all()
     assert int(d["n_early"]) == 3 and int(d["early_lattice"]) == 32
-    # 2048 in-flight updates on the 512 x 512 x 16 training slab.
-    assert abs(float(d["early_density"]) * 512 * 512 * 16 - 2048) < 1e-6
+    # 2048 in-flight updates on the 256 x 256 x 32 training grid.
+    shape = L.workload_shape(L.TRAIN_WORKLOAD)
+    assert abs(float(d["early_density"]) * float(np.prod(shape)) - 2048) < 1e-6
+    assert str(d["train_seeds"]) == "100:132"
     assert abs(float(d["s_in"]) - L.S_IN) < 1e-6 and abs(float(d["s_out"]) - L.S_OUT) < 1e-4
