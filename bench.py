@@ -170,11 +170,12 @@ def run_ours(args, rank, world, dist):
         opts, trials = rc.autotune(ssm, opts, probe_iters=2)
         tune = {"chosen": {"warps_per_voxel": opts.warps_per_voxel, "warps_in_flight": opts.warps_in_flight,
                            "entries_per_lane": opts.entries_per_lane, "lattice": opts.lattice,
-                           "stage_column": opts.stage_column},
+                           "stage_column": opts.stage_column, "entry_pairs": opts.entry_pairs},
                 "trials": [[t["warps_per_voxel"], t["warps_in_flight"], t["entries_per_lane"], t["lattice"],
-                            t["stage_column"], round(t["device_ms"], 1), round(t["score"], 1)] for t in trials],
+                            t["stage_column"], t["entry_pairs"], round(t["device_ms"], 1), round(t["score"], 1)]
+                           for t in trials],
                 "trial_fields": ["warps_per_voxel", "warps_in_flight", "entries_per_lane", "lattice",
-                                 "stage_column", "ms_2_iterations", "cost_decrease_per_ms"]}
+                                 "stage_column", "entry_pairs", "ms_2_iterations", "cost_decrease_per_ms"]}
         rc.set_volume(ssm, None)
 
     rc.iterate(ssm, args.warmup, opts)

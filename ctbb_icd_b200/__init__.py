@@ -360,7 +360,8 @@ class Recon:
         check(lib().ctbb_gpu_recon_autotune(self.handle, ssm.handle, C.byref(opts or icd_opts()),
                                             int(probe_iters), C.byref(best), C.byref(rep)))
         trials = [dict(warps_in_flight=t.warps_in_flight, warps_per_voxel=t.warps_per_voxel,
-                       entries_per_lane=t.entries_per_lane, stage_column=t.stage_column, lattice=t.lattice,
+                       entries_per_lane=t.entries_per_lane, stage_column=t.stage_column,
+                       entry_pairs=t.entry_pairs, lattice=t.lattice,
                        device_ms=t.device_ms,
                        cost=t.cost, score=t.score, best=(i == rep.best))
                   for i, t in enumerate(rep.trials[:rep.n_trials])]

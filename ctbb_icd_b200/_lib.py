@@ -108,7 +108,7 @@ class IcdOpts(C.Structure):
 
 class TuneTrial(C.Structure):
     _fields_ = [("warps_in_flight", _I), ("warps_per_voxel", _I), ("lattice", _I), ("entries_per_lane", _I),
-                ("stage_column", _I), ("reserved", _I), ("device_ms", _D), ("cost", _D), ("score", _D)]
+                ("stage_column", _I), ("entry_pairs", _I), ("device_ms", _D), ("cost", _D), ("score", _D)]
 
 
 class TuneReport(C.Structure):

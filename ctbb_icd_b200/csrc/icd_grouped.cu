@@ -479,26 +479,29 @@ __global__ void __launch_bounds__(256) icd_grouped_kernel(GParams P, const uint3
 }
 
 // One warp per update over the matrix's entry pairs (the streamed kernel's
-// order, stack start view and round trips; the pair form halves the matrix
-// loads and reads 4 bytes per entry instead of 6). Lane l takes pairs
-// m, m + 32, ... of a chunk of 32 x U pairs; each pair is one 8-byte load and
-// one or two e gathers.
-template <int U>
-__device__ __forceinline__ void load_pairs(const uint2* __restrict__ pairs, int64_t m, int64_t en, int off,
-                                           uint64_t pol, int* q, uint32_t* wp) {
+// order, stack start view and round trips). Lanes 2j and 2j+1 share pair j of
+// a row of 16 pairs: both load the same 8 bytes (one request) and each takes
+// one of its two entries, so a warp's gathers touch consecutive sinogram
+// rows as with single entries (coalesced in the same sectors) while the
+// matrix costs 4 bytes per entry instead of 6. Position p of a lane in row u
+// of a chunk: pair base + 16 u + lane / 2, entry lane & 1.
+template <int U, int STRIDE = 16>
+__device__ __forceinline__ void load_pair_entries(const uint2* __restrict__ pairs, int64_t m, int64_t en, int off,
+                                                  int half, uint64_t pol, int* q, float* wt) {
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int64_t mu = m + 32 * u;
+        const int64_t mu = m + (int64_t)STRIDE * u;
+        q[u] = -1;
+        wt[u] = 0.f;
         if (mu < en) {
             uint32_t a, bb;
             asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
                          : "=r"(a), "=r"(bb)
                          : "l"(pairs + mu), "l"(pol));
-            q[u] = (int)a + off;
-            wp[u] = bb;
-        } else {
-            q[u] = -1;
-            wp[u] = 0u;
+            if (!half || (bb >> 16)) {
+                q[u] = (int)a + off + half;
+                wt[u] = half ? half_hi(bb) : half_lo(bb);
+            }
         }
     }
 }
@@ -507,26 +510,21 @@ template <int U>
 __device__ __forceinline__ void gather_pairs(const uint2* __restrict__ pairs, const float* e, int64_t b, int64_t en,
                                              int off, int lane, uint64_t pol, float& acc_b, float& acc_a) {
     if (b >= en) return;
+    const int half = lane & 1, j = lane >> 1;
     int qa[U];
-    uint32_t wa[U];
-    load_pairs<U>(pairs, b + lane, en, off, pol, qa, wa);
-    for (int64_t base = b; base < en; base += 32 * U) {
-        float e0[U], e1[U];
+    float wa[U];
+    load_pair_entries<U>(pairs, b + j, en, off, half, pol, qa, wa);
+    for (int64_t base = b; base < en; base += 16 * U) {
+        float ev[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            e0[u] = qa[u] >= 0 ? __ldcg(e + qa[u]) : 0.f;
-            e1[u] = (qa[u] >= 0 && (wa[u] >> 16)) ? __ldcg(e + qa[u] + 1) : 0.f;
-        }
+        for (int u = 0; u < U; ++u) ev[u] = qa[u] >= 0 ? __ldcg(e + qa[u]) : 0.f;
         int qb[U];
-        uint32_t wb[U];
-        load_pairs<U>(pairs, base + 32 * U + lane, en, off, pol, qb, wb);
+        float wb[U];
+        load_pair_entries<U>(pairs, base + 16 * U + j, en, off, half, pol, qb, wb);
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const float w0 = half_lo(wa[u]), w1 = half_hi(wa[u]);
-            acc_b = fmaf(w0, e0[u], acc_b);
-            acc_b = fmaf(w1, e1[u], acc_b);
-            acc_a = fmaf(w0, w0, acc_a);
-            acc_a = fmaf(w1, w1, acc_a);
+            acc_b = fmaf(wa[u], ev[u], acc_b);
+            acc_a = fmaf(wa[u], wa[u], acc_a);
             qa[u] = qb[u];
             wa[u] = wb[u];
         }
@@ -537,17 +535,15 @@ template <int U>
 __device__ __forceinline__ void scatter_pairs(const uint2* __restrict__ pairs, float* e, int64_t b, int64_t en,
                                               int off, int lane, uint64_t pol, float du) {
     if (b >= en) return;
-    const int64_t nchunk = (en - b + 32 * U - 1) / (32 * U);
+    const int half = lane & 1, j = lane >> 1;
+    const int64_t nchunk = (en - b + 16 * U - 1) / (16 * U);
     for (int64_t c = nchunk - 1; c >= 0; --c) {
         int qs[U];
-        uint32_t ws[U];
-        load_pairs<U>(pairs, b + c * (32 * U) + lane, en, off, pol, qs, ws);
+        float ws[U];
+        load_pair_entries<U>(pairs, b + c * (16 * U) + j, en, off, half, pol, qs, ws);
 #pragma unroll
         for (int u = 0; u < U; ++u)
-            if (qs[u] >= 0) {
-                atomicAdd(e + qs[u], -du * half_lo(ws[u]));
-                if (ws[u] >> 16) atomicAdd(e + qs[u] + 1, -du * half_hi(ws[u]));
-            }
+            if (qs[u] >= 0) atomicAdd(e + qs[u], -du * ws[u]);
     }
 }
 
@@ -629,24 +625,27 @@ __device__ __forceinline__ void load_seq(const int32_t* __restrict__ idx, const 
 
 // One voxel update per CTA of WPV warps over the matrix's entry pairs
 // ({q, w0 | w1 << 16}: rows q and q + 1 of one (view, channel), w1 = 0 for a
-// lone entry). Each thread keeps R pairs (2R entries) in registers from the
-// gather to the scatter, so a column of up to 2 * 32 * WPV * R entries is
-// read from HBM once; longer columns re-read their tail. Same update as
-// icd_cta_kernel; the entry counts (for the statistics) come from the entry
-// offsets.
-
+// lone entry). Threads 2j and 2j+1 share pair j (one 8-byte request) and
+// take one entry each, so the gathers stay coalesced as with single entries;
+// each thread keeps R entries in registers from the gather to the scatter, so
+// a column of up to 32 * WPV * R / 2 pairs is read from HBM once; longer
+// columns re-read their tail. Same update as icd_cta_kernel; the entry
+// counts (for the statistics) come from the entry offsets.
 template <int WPV, int R>
 __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
     GParams P, const uint32_t* __restrict__ order, const int64_t* __restrict__ pcolptr,
     const uint32_t* __restrict__ pvptr, const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
     const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue, unsigned long long* stats) {
     constexpr int NT = 32 * WPV;
-    constexpr int64_t CAP = (int64_t)NT * R;
+    constexpr int NP = NT / 2;  // pairs per row of the CTA
+    constexpr int64_t CAP = (int64_t)NP * R;
     unsigned long long n_ent = 0, n_upd = 0;
     __shared__ unsigned long long s_item;
     __shared__ float s_red[2 * WPV + 1];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int half = tid & 1, j = tid >> 1;
     const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint64_t pol = l2_keep();
     for (;;) {
         if (tid == 0) s_item = atomicAdd(queue, 1ull);
         __syncthreads();
@@ -669,60 +668,48 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
         const int off = s * P.nch * P.nr;
         const int64_t e0 = min(en, b + CAP);
         int qr[R];
-        uint32_t wr[R];
+        float wr[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int64_t m = b + tid + (int64_t)NT * r;
+            const int64_t m = b + j + (int64_t)NP * r;
+            qr[r] = -1;
+            wr[r] = 0.f;
             if (m < e0) {
                 const uint2 pr = __ldg(pairs + m);
-                qr[r] = (int)pr.x + off;
-                wr[r] = pr.y;
-            } else {
-                qr[r] = -1;
-                wr[r] = 0u;
+                if (!half || (pr.y >> 16)) {
+                    qr[r] = (int)pr.x + off + half;
+                    wr[r] = half ? half_hi(pr.y) : half_lo(pr.y);
+                }
             }
         }
         float acc_b = 0.f, acc_a = 0.f;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            float ev0 = 0.f, ev1 = 0.f;
-            if (qr[r] >= 0) {
-                ev0 = __ldcg(e + qr[r]);
-                if (wr[r] >> 16) ev1 = __ldcg(e + qr[r] + 1);
-            }
-            const float w0 = half_lo(wr[r]), w1 = half_hi(wr[r]);
-            acc_b = fmaf(w0, ev0, acc_b);
-            acc_b = fmaf(w1, ev1, acc_b);
-            acc_a = fmaf(w0, w0, acc_a);
-            acc_a = fmaf(w1, w1, acc_a);
+            const float ev = qr[r] >= 0 ? __ldcg(e + qr[r]) : 0.f;
+            acc_b = fmaf(wr[r], ev, acc_b);
+            acc_a = fmaf(wr[r], wr[r], acc_a);
         }
-        for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+        for (int64_t base = e0; base < en; base += (int64_t)NP * kU) {
             int qo[kU];
-            uint32_t wo[kU];
+            float wo[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int64_t m = base + tid + (int64_t)NT * u;
+                const int64_t m = base + j + (int64_t)NP * u;
+                qo[u] = -1;
+                wo[u] = 0.f;
                 if (m < en) {
                     const uint2 pr = __ldg(pairs + m);
-                    qo[u] = (int)pr.x + off;
-                    wo[u] = pr.y;
-                } else {
-                    qo[u] = -1;
-                    wo[u] = 0u;
+                    if (!half || (pr.y >> 16)) {
+                        qo[u] = (int)pr.x + off + half;
+                        wo[u] = half ? half_hi(pr.y) : half_lo(pr.y);
+                    }
                 }
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                float ev0 = 0.f, ev1 = 0.f;
-                if (qo[u] >= 0) {
-                    ev0 = __ldcg(e + qo[u]);
-                    if (wo[u] >> 16) ev1 = __ldcg(e + qo[u] + 1);
-                }
-                const float w0 = half_lo(wo[u]), w1 = half_hi(wo[u]);
-                acc_b = fmaf(w0, ev0, acc_b);
-                acc_b = fmaf(w1, ev1, acc_b);
-                acc_a = fmaf(w0, w0, acc_a);
-                acc_a = fmaf(w1, w1, acc_a);
+                const float ev = qo[u] >= 0 ? __ldcg(e + qo[u]) : 0.f;
+                acc_b = fmaf(wo[u], ev, acc_b);
+                acc_a = fmaf(wo[u], wo[u], acc_a);
             }
         }
         acc_b = warp_sum(acc_b);
@@ -752,20 +739,14 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
         if (du != 0.f) {
 #pragma unroll
             for (int r = 0; r < R; ++r)
-                if (qr[r] >= 0) {
-                    atomicAdd(e + qr[r], -du * half_lo(wr[r]));
-                    if (wr[r] >> 16) atomicAdd(e + qr[r] + 1, -du * half_hi(wr[r]));
-                }
-            for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+                if (qr[r] >= 0) atomicAdd(e + qr[r], -du * wr[r]);
+            for (int64_t base = e0; base < en; base += (int64_t)NP * kU) {
+                int qo[kU];
+                float wo[kU];
+                load_pair_entries<kU, NP>(pairs, base + j, en, off, half, pol, qo, wo);
 #pragma unroll
-                for (int u = 0; u < kU; ++u) {
-                    const int64_t m = base + tid + (int64_t)NT * u;
-                    if (m < en) {
-                        const uint2 pr = __ldg(pairs + m);
-                        atomicAdd(e + ((int)pr.x + off), -du * half_lo(pr.y));
-                        if (pr.y >> 16) atomicAdd(e + ((int)pr.x + off + 1), -du * half_hi(pr.y));
-                    }
-                }
+                for (int u = 0; u < kU; ++u)
+                    if (qo[u] >= 0) atomicAdd(e + qo[u], -du * wo[u]);
             }
             n_ent += (unsigned long long)n_entries;
             ++n_upd;
@@ -1721,11 +1702,11 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
         } else if (pairs) {
             const int blocks = (int)in_flight;
             if (wpv == 8)
-                icd_cta_pairs_kernel<8, 16><<<blocks, 256, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                icd_cta_pairs_kernel<8, 32><<<blocks, 256, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
                                                                    ssm->d_pairs, vp, rc->d_start, rc->d_e32,
                                                                    rc->d_x32, ctx->d_queue, stats);
             else
-                icd_cta_pairs_kernel<4, 16><<<blocks, 128, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                icd_cta_pairs_kernel<4, 32><<<blocks, 128, 0, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
                                                                    ssm->d_pairs, vp, rc->d_start, rc->d_e32,
                                                                    rc->d_x32, ctx->d_queue, stats);
         } else {

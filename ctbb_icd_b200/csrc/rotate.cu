@@ -2,10 +2,11 @@
 //
 // Replaces rotate_slices_rotating2fixed (rotate_slices.cpp:81-114),
 // rotate_slices_fixed2rotating (:48-79), rotate_slice (:116-154) and interp2
-// (interp.h:41-76). Each CTA writes a 32 x 32 output tile: it loads the
-// input box the tile's bilinear taps fall in (at most ~48 x 48 pixels) into
-// shared memory with coalesced row reads and interpolates from there, so the
-// kernel streams each slice in and out once, bounded by HBM bandwidth.
+// (interp.h:41-76). Each thread gathers the four bilinear taps of four
+// output pixels of one row, all loads issued before any is used. (A variant
+// that staged each 32 x 32 output tile's input box in shared memory measured
+// slower: at 134 MB per volume the kernel is bound by its per-pixel
+// arithmetic and launch, not by HBM.)
 //
 // Compiled with -fmad=false. The per-slice cos/sin are computed on the host
 // with the reference's expressions, the rotated coordinates in double and
@@ -23,117 +24,61 @@
 
 namespace {
 
-// Output tile of kTile x kTile pixels per CTA of kTile x kRows threads
-// (each thread kTile / kRows rows). The input pixels the tile's taps read lie
-// in a box of at most (kTile * sqrt(2) + 3)^2: it is loaded into shared
-// memory once with coalesced row reads, and the four taps of every pixel
-// come from there.
-constexpr int kTile = 32, kRows = 8, kRotPix = kTile / kRows;
-constexpr int kBoxCap = 52 * 52;  // floats; a larger box (never for kTile 32) reads from global
+// Output pixels per thread (spaced kRotBlock apart along x).
+constexpr int kRotBlock = 128, kRotPix = 4;
 
-// FLOAT_CENTRE: the centre (cvx, cvy) is exactly a float. Then
+// Grid: x = groups of kRotBlock * kRotPix pixels of a row, y = row, z = slice.
+// Each thread issues the 16 bilinear loads of its 4 pixels before using any
+// (the input slice, at most 1 MB at 512 x 512, stays in L2 while its rows are
+// written). FLOAT_CENTRE: the centre (cvx, cvy) is exactly a float. Then
 // (float)((double)xp + cvx) equals the float sum xp + (float)cvx: the exact
 // sum of two floats fits in a double's 53 bits unless the smaller one is
 // below about 2^-29 of the larger, and then it is far below half a float ulp
 // of the larger, so both roundings return the larger. The float add saves
-// two conversions per coordinate (they run on the narrow conversion pipe
-// that bounds this kernel).
+// two conversions per coordinate on the narrow conversion pipe.
 template <bool FLOAT_CENTRE>
-__global__ void __launch_bounds__(kTile * kRows) rotate_kernel(const float* __restrict__ in, float* __restrict__ out,
-                                                               int nx, int ny, int nz, int dim1, int dim2,
-                                                               int out_stride_y, const double* __restrict__ cs,
-                                                               double cvx, double cvy) {
-    __shared__ float box[kBoxCap];
-    __shared__ int s_lim[4];  // min f1, max f1 + 1, min f2, max f2 + 1 over the tile's in-range taps
-    const int k = blockIdx.z;
-    const int tx = threadIdx.x % kTile, ty = threadIdx.x / kTile;
-    const int x_idx = blockIdx.x * kTile + tx;
+__global__ void __launch_bounds__(kRotBlock) rotate_kernel(const float* __restrict__ in, float* __restrict__ out,
+                                                           int nx, int ny, int nz, int dim1, int dim2,
+                                                           int out_stride_y, const double* __restrict__ cs,
+                                                           double cvx, double cvy) {
+    const int k = blockIdx.z, y_idx = blockIdx.y;
     const uint64_t npix = (uint64_t)nx * ny;
     const double c = cs[2 * k], s = cs[2 * k + 1];
     const float* a = in + (uint64_t)k * npix;
-    if (threadIdx.x == 0) {
-        s_lim[0] = INT_MAX;
-        s_lim[1] = INT_MIN;
-        s_lim[2] = INT_MAX;
-        s_lim[3] = INT_MIN;
-    }
-    __syncthreads();
-    float vv[kRotPix], ww[kRotPix];
-    int f1s[kRotPix], f2s[kRotPix];
-    bool inside[kRotPix];
-    int lo1 = INT_MAX, hi1 = INT_MIN, lo2 = INT_MAX, hi2 = INT_MIN;
-    const double x = x_idx - cvx;
-    const double cx = c * x, sx = s * x;
+    const double y = y_idx - cvy;
+    const double sy = s * y, cy = c * y;
     const float cvx_f = (float)cvx, cvy_f = (float)cvy;
+    float tap[kRotPix][4], vv[kRotPix], ww[kRotPix];
+    bool inside[kRotPix];
 #pragma unroll
     for (int u = 0; u < kRotPix; ++u) {
-        const int y_idx = blockIdx.y * kTile + ty + u * kRows;
-        const double y = y_idx - cvy;
-        const float xp = (float)(cx - s * y);
-        const float yp = (float)(sx + c * y);
+        const int x_idx = blockIdx.x * (kRotBlock * kRotPix) + u * kRotBlock + threadIdx.x;
+        const double x = x_idx - cvx;
+        const float xp = (float)(c * x - sy);
+        const float yp = (float)(s * x + cy);
         const float i1 = FLOAT_CENTRE ? __fadd_rn(xp, cvx_f) : (float)((double)xp + cvx);
         const float i2 = FLOAT_CENTRE ? __fadd_rn(yp, cvy_f) : (float)((double)yp + cvy);
         // interp.h:57-58: zero outside [0, n-2] in either index.
-        inside[u] = x_idx < nx && y_idx < ny &&
-                    !(i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0));
+        inside[u] = x_idx < nx && !(i1 > (float)(dim1 - 2) || (i1 < 0) || i2 > (float)(dim2 - 2) || (i2 < 0));
         vv[u] = i1 - floorf(i1);
         ww[u] = i2 - floorf(i2);
-        f1s[u] = inside[u] ? (int)floorf(i1) : 0;
-        f2s[u] = inside[u] ? (int)floorf(i2) : 0;
         if (inside[u]) {
-            lo1 = min(lo1, f1s[u]);
-            hi1 = max(hi1, f1s[u] + 1);
-            lo2 = min(lo2, f2s[u]);
-            hi2 = max(hi2, f2s[u] + 1);
+            const int f1 = (int)floorf(i1), f2 = (int)floorf(i2);
+            tap[u][0] = __ldg(a + (f2 * dim1 + f1));
+            tap[u][1] = __ldg(a + (f2 * dim1 + f1 + 1));
+            tap[u][2] = __ldg(a + ((f2 + 1) * dim1 + f1));
+            tap[u][3] = __ldg(a + ((f2 + 1) * dim1 + f1 + 1));
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        lo1 = min(lo1, __shfl_xor_sync(0xffffffffu, lo1, o));
-        hi1 = max(hi1, __shfl_xor_sync(0xffffffffu, hi1, o));
-        lo2 = min(lo2, __shfl_xor_sync(0xffffffffu, lo2, o));
-        hi2 = max(hi2, __shfl_xor_sync(0xffffffffu, hi2, o));
-    }
-    if ((threadIdx.x & 31) == 0 && lo1 <= hi1) {
-        atomicMin(&s_lim[0], lo1);
-        atomicMax(&s_lim[1], hi1);
-        atomicMin(&s_lim[2], lo2);
-        atomicMax(&s_lim[3], hi2);
-    }
-    __syncthreads();
-    const int bx0 = s_lim[0], by0 = s_lim[2];
-    const int bw = s_lim[1] - bx0 + 1, bh = s_lim[3] - by0 + 1;
-    const bool staged = s_lim[0] <= s_lim[1] && bw * bh <= kBoxCap;
-    if (staged) {
-        // Rows of the box, coalesced along x (taps lie in [0, dim - 1]).
-        for (int r = ty; r < bh; r += kRows)
-            for (int q = tx; q < bw; q += kTile) box[r * bw + q] = __ldg(a + ((by0 + r) * dim1 + bx0 + q));
-    }
-    __syncthreads();
 #pragma unroll
     for (int u = 0; u < kRotPix; ++u) {
-        const int y_idx = blockIdx.y * kTile + ty + u * kRows;
-        if (x_idx >= nx || y_idx >= ny) continue;
-        float val = 0.0f;
-        if (inside[u]) {
-            float t0, t1, t2, t3;
-            if (staged) {
-                const int o = (f2s[u] - by0) * bw + (f1s[u] - bx0);
-                t0 = box[o];
-                t1 = box[o + 1];
-                t2 = box[o + bw];
-                t3 = box[o + bw + 1];
-            } else {
-                const int f1 = f1s[u], f2 = f2s[u];
-                t0 = __ldg(a + (f2 * dim1 + f1));
-                t1 = __ldg(a + (f2 * dim1 + f1 + 1));
-                t2 = __ldg(a + ((f2 + 1) * dim1 + f1));
-                t3 = __ldg(a + ((f2 + 1) * dim1 + f1 + 1));
-            }
-            const float v = vv[u], w = ww[u];
-            // interp.h:70-73, the reference's operation order.
-            val = t0 * (1.0f - v) * (1.0f - w) + t1 * v * (1.0f - w) + t2 * (1.0f - v) * w + t3 * v * w;
-        }
+        const int x_idx = blockIdx.x * (kRotBlock * kRotPix) + u * kRotBlock + threadIdx.x;
+        if (x_idx >= nx) continue;
+        const float v = vv[u], w = ww[u];
+        // interp.h:70-73, the reference's operation order.
+        const float val = inside[u] ? tap[u][0] * (1.0f - v) * (1.0f - w) + tap[u][1] * v * (1.0f - w) +
+                                          tap[u][2] * (1.0f - v) * w + tap[u][3] * v * w
+                                    : 0.0f;
         // rotate_slices.cpp:128 writes with stride num_voxels_y.
         out[(uint64_t)k * npix + (uint64_t)x_idx + (uint64_t)y_idx * out_stride_y] = val;
     }
@@ -144,13 +89,13 @@ __global__ void __launch_bounds__(kTile * kRows) rotate_kernel(const float* __re
 cudaError_t launch_rotate(cudaStream_t st, const ctbb_geom_c& g, const float* in, float* out, const double* cs) {
     const uint64_t npix = g.num_voxels_x * g.num_voxels_y;
     if (npix == 0 || g.num_voxels_z == 0) return cudaSuccess;
-    const unsigned gx = (unsigned)((g.num_voxels_x + kTile - 1) / kTile);
-    const unsigned gy = (unsigned)((g.num_voxels_y + kTile - 1) / kTile);
+    const unsigned gx = (unsigned)((g.num_voxels_x + kRotBlock * kRotPix - 1) / (kRotBlock * kRotPix));
+    const bool fc = (double)(float)g.center_voxel_x == g.center_voxel_x &&
+                    (double)(float)g.center_voxel_y == g.center_voxel_y;
     for (uint64_t k0 = 0; k0 < g.num_voxels_z; k0 += 65535) {
         const unsigned nz = (unsigned)std::min<uint64_t>(65535, g.num_voxels_z - k0);
-        const bool fc = (double)(float)g.center_voxel_x == g.center_voxel_x &&
-                        (double)(float)g.center_voxel_y == g.center_voxel_y;
-        (fc ? rotate_kernel<true> : rotate_kernel<false>)<<<dim3(gx, gy, nz), kTile * kRows, 0, st>>>(
+        (fc ? rotate_kernel<true> : rotate_kernel<false>)<<<dim3(gx, (unsigned)g.num_voxels_y, nz), kRotBlock, 0,
+                                                          st>>>(
             in + k0 * npix, out + k0 * npix, (int)g.num_voxels_x, (int)g.num_voxels_y, (int)nz, (int)g.nx, (int)g.ny,
             (int)g.num_voxels_y, cs + 2 * k0, g.center_voxel_x, g.center_voxel_y);
         const cudaError_t e = cudaGetLastError();

@@ -59,33 +59,36 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     const int sms = rc->ctx->sm_count;
     const int wmax = sms * 48;
     struct Cand {
-        int wpv, w, epl, half, stage;
+        int wpv, w, epl, half, stage, pairs;  // pairs: entry_pairs (0 pairs with FP16, -1 single entries)
     };
     std::vector<Cand> cands;
     // Lockstep stacks: two CTAs of 16 updates per SM with 8 entries per lane
     // in flight. (One CTA with 16 entries per lane measured about twice as
     // slow on the 512 x 512 x 64 workload and is not probed.)
-    cands.push_back({1, 2 * 16 * sms, 8, 0, 3});
+    cands.push_back({1, 2 * 16 * sms, 8, 0, 3, 0});
     // Shared-memory staged kernels: one CTA per SM with 4 (or 8) updates,
     // the matrix read once per update.
     for (int epl : {16, 8}) {
-        cands.push_back({1, 4 * sms, epl, 0, 1});
-        cands.push_back({1, 8 * sms, epl, 0, 2});
+        cands.push_back({1, 4 * sms, epl, 0, 1, 0});
+        cands.push_back({1, 8 * sms, epl, 0, 2, 0});
     }
-    cands.push_back({1, 4 * sms, 16, 1, 1});
+    cands.push_back({1, 4 * sms, 16, 1, 1, 0});
     for (int epl : {8, 16})
         for (int m4 : {1, 2, 4, 8}) {
             const int w = std::max(32, std::min(wmax, w0 * m4 / 4));
-            cands.push_back({1, w, epl, 0, 0});
-            if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1, 0});
+            cands.push_back({1, w, epl, 0, 0, 0});
+            if (m4 == 4 && epl == 8) cands.push_back({1, w, epl, 1, 0, 0});
+            // the same shape over single entries (FP16 weights read as pairs above)
+            if (m4 == 4 && epl == 16 && o.weights == CTBB_SSM_FP16) cands.push_back({1, w, epl, 0, 0, -1});
         }
     // Several warps per update (the column's entries, or entry pairs with
     // FP16 weights, kept in registers): four or eight updates per SM.
-    cands.push_back({4, 4 * sms * 4, 8, 0, 0});
-    cands.push_back({4, 8 * sms * 4, 8, 0, 0});
-    cands.push_back({8, 4 * sms * 8, 8, 0, 0});
+    cands.push_back({4, 4 * sms * 4, 8, 0, 0, 0});
+    if (o.weights == CTBB_SSM_FP16) cands.push_back({4, 4 * sms * 4, 8, 0, 0, -1});
+    cands.push_back({4, 8 * sms * 4, 8, 0, 0, 0});
+    cands.push_back({8, 4 * sms * 8, 8, 0, 0, 0});
     struct Trial {
-        int wpv, w, epl, t, stage;
+        int wpv, w, epl, t, stage, pairs;
         double ms, cost, score;
     };
     std::vector<Trial> trials;
@@ -98,6 +101,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             c.warps_per_voxel = cd.wpv;
             c.entries_per_lane = cd.epl;
             c.stage_column = cd.stage;
+            c.entry_pairs = cd.pairs;
             c.lattice = 0;
             const int t_auto = lattice_spacing(rc, c);
             c.lattice = cd.half ? std::max(4, t_auto / 2) : t_auto;
@@ -109,7 +113,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             bool seen = false;
             for (const Trial& tr : trials)
                 seen |= tr.wpv == c.warps_per_voxel && tr.w == c.warps_in_flight && tr.t == c.lattice &&
-                        tr.epl == c.entries_per_lane && tr.stage == c.stage_column;
+                        tr.epl == c.entries_per_lane && tr.stage == c.stage_column && tr.pairs == c.entry_pairs;
             if (seen) continue;
             if (copy(rc->d_x32, d_xs, rc->d_e32, d_es) != cudaSuccess) {
                 status = fail(CTBB_ERR_CUDA, "autotune restore");
@@ -128,7 +132,8 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             if (status != CTBB_OK) break;
             const double score = (c0 - cost) / std::max(ms_tot, 1e-3);
             trials.push_back(
-                {c.warps_per_voxel, c.warps_in_flight, c.entries_per_lane, c.lattice, c.stage_column, ms_tot, cost, score});
+                {c.warps_per_voxel, c.warps_in_flight, c.entries_per_lane, c.lattice, c.stage_column, c.entry_pairs,
+                 ms_tot, cost, score});
             if (ibest < 0 || score > trials[ibest].score) ibest = (int)trials.size() - 1;
         }
     }
@@ -144,6 +149,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     best->warps_per_voxel = trials[ibest].wpv;
     best->entries_per_lane = trials[ibest].epl;
     best->stage_column = trials[ibest].stage;
+    best->entry_pairs = trials[ibest].pairs;
     best->lattice = trials[ibest].t;
     if (report) {
         memset(report, 0, sizeof(*report));
@@ -155,6 +161,7 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             report->trials[i].warps_per_voxel = trials[i].wpv;
             report->trials[i].entries_per_lane = trials[i].epl;
             report->trials[i].stage_column = trials[i].stage;
+            report->trials[i].entry_pairs = trials[i].pairs;
             report->trials[i].lattice = trials[i].t;
             report->trials[i].device_ms = trials[i].ms;
             report->trials[i].cost = trials[i].cost;

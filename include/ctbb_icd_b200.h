@@ -481,7 +481,7 @@ typedef struct ctbb_tune_trial {
     int32_t lattice;
     int32_t entries_per_lane;
     int32_t stage_column;
-    int32_t reserved;
+    int32_t entry_pairs;
     double device_ms;   /* ICD kernel time of the probe iterations */
     double cost;        /* FP64 cost after them                    */
     double score;       /* (start_cost - cost) / device_ms         */

@@ -199,8 +199,10 @@ def test_autotune_leaves_iterate_and_picks_a_candidate(ctx):
     assert (best.warps_in_flight, best.warps_per_voxel, best.lattice, best.entries_per_lane) == (
         chosen[0]["warps_in_flight"], chosen[0]["warps_per_voxel"], chosen[0]["lattice"],
         chosen[0]["entries_per_lane"])
-    assert {t["warps_per_voxel"] for t in trials} == {1, 4}
+    assert {t["warps_per_voxel"] for t in trials} == {1, 4, 8}
     assert {t["entries_per_lane"] for t in trials} == {8, 16}
+    assert {t["stage_column"] for t in trials} == {0, 1, 2, 3}
+    assert best.entry_pairs == chosen[0]["entry_pairs"]
     # Every launch stays within the visiting order's concurrency bound.
     n = scan.rc.volume().size
     assert all(t["warps_in_flight"] // t["warps_per_voxel"] <= max(1, n // t["lattice"] ** 2) for t in trials)

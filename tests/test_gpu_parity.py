@@ -237,11 +237,11 @@ def test_entry_pairs_match_single_entries(ctx, converged_cfg1_small, wpv):
                                       warps_in_flight=wpv, entry_pairs=pairs))
         out[pairs] = rc.volume_f64()
         rc.free()
-    assert ssm.info().n_pairs > 0
-    # every run of the z interpolation is two rows: about half as many pairs as entries
-    assert abs(ssm.info().n_pairs - ssm.info().nnz / 2) <= 0.01 * ssm.info().nnz
     a, b = out[0], out[-1]
     assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), np.linalg.norm(a - b) / np.linalg.norm(b)
+    # runs of two detector rows make most pairs (a lone entry takes a pair too)
+    info = ssm.info()
+    assert info.nnz / 2 <= info.n_pairs <= 0.75 * info.nnz, (info.n_pairs, info.nnz)
 
 
 def test_batch_of_uneven_scans_converges(ctx, converged_cfg1_small, tmp_path):
