@@ -161,7 +161,8 @@ def run_ours(args, rank, world, dist):
     setup_s = time.time() - t0
     info = ssm.info()
     opts = C.icd_opts(mode=C.ICD_GROUPED, weights=weights_fmt, warps_in_flight=args.warps, lattice=args.lattice,
-                      warps_per_voxel=args.wpv, entries_per_lane=args.epl, stage_column=max(0, args.stage_column))
+                      warps_per_voxel=args.wpv, entries_per_lane=args.epl, stage_column=max(0, args.stage_column),
+                      entry_pairs=args.entry_pairs, stack_align=args.stack_align, l2_hints=args.l2_hints)
     nvox = int(np.prod(rp.shape))
     tune = None
     if args.autotune:
@@ -211,8 +212,9 @@ def run_ours(args, rank, world, dist):
     # The matrix in the form the kernel reads: entry pairs (8 B per pair of
     # rows) when the iteration used them, else index + weight per entry.
     n_pairs = int(ssm.info().n_pairs)
-    uses_pairs = (n_pairs > 0 and weights_fmt == C.SSM_FP16 and opts.entry_pairs == 0
-                  and (opts.warps_per_voxel > 1 or opts.stage_column == 0))
+    uses_pairs = (n_pairs > 0 and weights_fmt == C.SSM_FP16
+                  and (opts.stage_column >= 4 or (opts.entry_pairs == 0
+                                                  and (opts.warps_per_voxel > 1 or opts.stage_column == 0))))
     ssm_read = 8.0 * n_pairs if uses_pairs else (4 + w_bytes) * float(info.nnz)
     b_iter = 4.0 * gathered + 4.0 * scattered + ssm_read + 8.0 * nvox
 
@@ -231,7 +233,8 @@ def run_ours(args, rank, world, dist):
         peak, peak_kind = measured_peak()
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
-        kernel = ("icd_lockstep_kernel" if opts.stage_column == 3 else
+        kernel = ("icd_bulk_kernel" if opts.stage_column >= 4 else
+                  "icd_lockstep_kernel" if opts.stage_column == 3 else
                   "icd_staged_kernel" if opts.stage_column else
                   "icd_grouped_pairs_kernel" if uses_pairs else "icd_grouped_kernel") \
             if opts.warps_per_voxel <= 1 else ("icd_cta_pairs_kernel" if uses_pairs else "icd_cta_kernel")
@@ -783,6 +786,14 @@ def main():
     ap.add_argument("--cnn-shape", type=int, nargs=3, default=[16, 256, 256])
     ap.add_argument("--cnn-engine", choices=["tcgen05", "mma_sync"], default="mma_sync",
                     help="--stage cnn: tensor-core path of the 32 -> 32 convolutions")
+    ap.add_argument("--entry-pairs", type=int, default=0, choices=[0, -1],
+                    help="with --no-autotune: 0 reads FP16 matrices as entry pairs, -1 as single entries")
+    ap.add_argument("--stack-align", type=int, default=0, choices=[0, 1],
+                    help="with --no-autotune, 4 or 8 warps per voxel: start each sweep at its slice stack's "
+                         "common data view")
+    ap.add_argument("--l2-hints", type=int, default=0, choices=[0, 1],
+                    help="with --no-autotune, 4 or 8 warps per voxel: matrix loads evict-first, e gathers "
+                         "evict-last")
     ap.add_argument("--stage-column", type=int, default=-1,
                     help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory, "
                          "3 sweeps each slice stack in lockstep in one CTA")

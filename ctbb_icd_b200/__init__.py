@@ -252,7 +252,8 @@ class Ssm:
 
 def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_flight=0, lattice=0,
              compute_cost=False, stop_rel_change=0.0, relax=0.0, priority=False,
-             warps_per_voxel=1, entries_per_lane=0, stage_column=0, entry_pairs=0) -> IcdOpts:
+             warps_per_voxel=1, entries_per_lane=0, stage_column=0, entry_pairs=0, stack_align=0,
+             l2_hints=0) -> IcdOpts:
     o = IcdOpts()
     o.mode, o.weights, o.refresh_every = int(mode), int(weights), int(refresh_every)
     o.warps_in_flight, o.lattice = int(warps_in_flight), int(lattice)
@@ -263,6 +264,8 @@ def icd_opts(mode=ICD_GROUPED, weights=SSM_FP32, refresh_every=0, warps_in_fligh
     o.entries_per_lane = int(entries_per_lane)
     o.stage_column = int(stage_column)
     o.entry_pairs = int(entry_pairs)
+    o.stack_align = int(stack_align)
+    o.l2_hints = int(l2_hints)
     return o
 
 

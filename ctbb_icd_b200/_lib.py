@@ -102,7 +102,7 @@ class IcdOpts(C.Structure):
         ("mode", _I), ("weights", _I), ("refresh_every", _I), ("warps_in_flight", _I),
         ("lattice", _I), ("compute_cost", _I), ("stop_rel_change", _D), ("relax", _D),
         ("priority", _I), ("warps_per_voxel", _I), ("entries_per_lane", _I), ("stage_column", _I),
-        ("entry_pairs", _I),
+        ("entry_pairs", _I), ("stack_align", _I), ("l2_hints", _I),
     ]
 
 

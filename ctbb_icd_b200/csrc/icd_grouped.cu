@@ -66,6 +66,8 @@ struct GParams {
     double lambda, delta;
     double relax;  // step scale applied to the exact 1-D update before the positivity clamp
     double cvx, cvy, vx, vy, fov_limit;
+    int stack_align;  // CTA kernels: sweep from the slice stack's common data view
+    int l2_hints;     // CTA kernels: matrix loads evict-first, e gathers evict-last
 };
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -105,6 +107,17 @@ __device__ __forceinline__ uint64_t l2_drop() {
     uint64_t p;
     asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
     return p;
+}
+__device__ __forceinline__ uint64_t l2_normal() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_normal.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// e gather through L2 (other SMs update e) with an eviction priority.
+__device__ __forceinline__ float ld_e(const float* p, uint64_t pol) {
+    float v;
+    asm volatile("ld.global.cg.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+    return v;
 }
 __device__ __forceinline__ int ld_idx(const int32_t* p, uint64_t pol) {
     int v;
@@ -150,6 +163,17 @@ __device__ __forceinline__ float half_hi(uint32_t w) { return __half2float(__ush
 
 constexpr int kU = 8;       // entries per lane in flight per chunk (default)
 constexpr int kStack = 16;  // same-parity slices that sweep the sinogram together
+
+// Matrix view where slice k's sweep starts so that the members of its slice
+// stack (up to kStack same-parity slices at one physical position) read and
+// update each sinogram sector at about the same time: the data view where
+// the stack's last member's window begins, clamped to k's window [v0, v1).
+__device__ __forceinline__ int stack_start_view(const GParams& P, const int32_t* __restrict__ start, int k, int s,
+                                                int v0, int v1) {
+    const int kl = min(k - (k % (2 * kStack)) + (k % 2) + 2 * (kStack - 1),
+                       ((k & 1) ? P.last_slice[1] : P.last_slice[0]));
+    return min(max(start[kl] - s, v0), v1);
+}
 
 // Gather beta += a e and alpha += a^2 over entries [b, en) of a column: chunks
 // of 32 x U entries, the next chunk's indices and weights fetched while this
@@ -506,6 +530,30 @@ __device__ __forceinline__ void load_pair_entries(const uint2* __restrict__ pair
     }
 }
 
+// Pair positions p, p + STRIDE, ... of an item's sweep: pair p + hi for
+// p < n1, else p + lo; -1 / 0 past n (the sweep's length).
+template <int U, int STRIDE>
+__device__ __forceinline__ void load_seq_pairs(const uint2* __restrict__ pairs, int p0, int n, int n1, int64_t hi,
+                                               int64_t lo, int off, int half, uint64_t pol, int* q, float* wt) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int p = p0 + STRIDE * u;
+        q[u] = -1;
+        wt[u] = 0.f;
+        if (p < n) {
+            const int64_t m = (p < n1 ? hi : lo) + p;
+            uint32_t a, bb;
+            asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                         : "=r"(a), "=r"(bb)
+                         : "l"(pairs + m), "l"(pol));
+            if (!half || (bb >> 16)) {
+                q[u] = (int)a + off + half;
+                wt[u] = half ? half_hi(bb) : half_lo(bb);
+            }
+        }
+    }
+}
+
 template <int U>
 __device__ __forceinline__ void gather_pairs(const uint2* __restrict__ pairs, const float* e, int64_t b, int64_t en,
                                              int off, int lane, uint64_t pol, float& acc_b, float& acc_a) {
@@ -629,10 +677,11 @@ __device__ __forceinline__ void load_seq(const int32_t* __restrict__ idx, const 
 // take one entry each, so the gathers stay coalesced as with single entries;
 // each thread keeps R entries in registers from the gather to the scatter, so
 // a column of up to 32 * WPV * R / 2 pairs is read from HBM once; longer
-// columns re-read their tail. Same update as icd_cta_kernel; the entry
-// counts (for the statistics) come from the entry offsets.
+// columns re-read their tail. Same update as icd_cta_kernel (including its
+// sweep order and L2 hints); the entry counts (for the statistics) come from
+// the entry offsets.
 template <int WPV, int R>
-__global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
+__global__ void __launch_bounds__(32 * WPV, 16 / WPV) icd_cta_pairs_kernel(
     GParams P, const uint32_t* __restrict__ order, const int64_t* __restrict__ pcolptr,
     const uint32_t* __restrict__ pvptr, const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
     const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue, unsigned long long* stats) {
@@ -645,7 +694,8 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const int half = tid & 1, j = tid >> 1;
     const uint64_t ncol = (uint64_t)P.nx * P.ny;
-    const uint64_t pol = l2_keep();
+    const uint64_t pol_m = P.l2_hints ? l2_drop() : l2_normal();
+    const uint64_t pol_e = P.l2_hints ? l2_keep() : l2_normal();
     for (;;) {
         if (tid == 0) s_item = atomicAdd(queue, 1ull);
         __syncthreads();
@@ -657,57 +707,54 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
         const int64_t q = (int64_t)col + (int64_t)ncol * k;
         const int s = start[k];
         const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
-        int64_t b = 0, en = 0, n_entries = 0;
+        int64_t b = 0, en = 0, mid = 0, n_entries = 0;
         if (v1 > v0) {
             const int64_t cb = pcolptr[col];
             const uint32_t* vp = pvptr + col * P.nvsm1;
             b = cb + vp[v0];
             en = cb + vp[v1];
+            mid = P.stack_align ? cb + vp[stack_start_view(P, start, k, s, v0, v1)] : b;
             if (tid == 0) n_entries = (int64_t)vptr[col * P.nvsm1 + v1] - (int64_t)vptr[col * P.nvsm1 + v0];
         }
         const int off = s * P.nch * P.nr;
-        const int64_t e0 = min(en, b + CAP);
+        // Sweep position p (pairs) -> pair p + hi for p < n1 ([mid, en)), else
+        // p + lo ([b, mid)).
+        const int n = (int)(en - b), n1 = (int)(en - mid);
+        const int64_t hi = mid, lo = b - n1;
+        const int nreg = min(n, (int)CAP);
         int qr[R];
         float wr[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int64_t m = b + j + (int64_t)NP * r;
+            const int p = j + NP * r;
             qr[r] = -1;
             wr[r] = 0.f;
-            if (m < e0) {
-                const uint2 pr = __ldg(pairs + m);
-                if (!half || (pr.y >> 16)) {
-                    qr[r] = (int)pr.x + off + half;
-                    wr[r] = half ? half_hi(pr.y) : half_lo(pr.y);
+            if (p < nreg) {
+                const int64_t m = (p < n1 ? hi : lo) + p;
+                uint32_t a, bb;
+                asm volatile("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;"
+                             : "=r"(a), "=r"(bb)
+                             : "l"(pairs + m), "l"(pol_m));
+                if (!half || (bb >> 16)) {
+                    qr[r] = (int)a + off + half;
+                    wr[r] = half ? half_hi(bb) : half_lo(bb);
                 }
             }
         }
         float acc_b = 0.f, acc_a = 0.f;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const float ev = qr[r] >= 0 ? __ldcg(e + qr[r]) : 0.f;
+            const float ev = qr[r] >= 0 ? ld_e(e + qr[r], pol_e) : 0.f;
             acc_b = fmaf(wr[r], ev, acc_b);
             acc_a = fmaf(wr[r], wr[r], acc_a);
         }
-        for (int64_t base = e0; base < en; base += (int64_t)NP * kU) {
+        for (int base = (int)CAP; base < n; base += NP * kU) {
             int qo[kU];
             float wo[kU];
+            load_seq_pairs<kU, NP>(pairs, base + j, n, n1, hi, lo, off, half, pol_m, qo, wo);
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int64_t m = base + j + (int64_t)NP * u;
-                qo[u] = -1;
-                wo[u] = 0.f;
-                if (m < en) {
-                    const uint2 pr = __ldg(pairs + m);
-                    if (!half || (pr.y >> 16)) {
-                        qo[u] = (int)pr.x + off + half;
-                        wo[u] = half ? half_hi(pr.y) : half_lo(pr.y);
-                    }
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < kU; ++u) {
-                const float ev = qo[u] >= 0 ? __ldcg(e + qo[u]) : 0.f;
+                const float ev = qo[u] >= 0 ? ld_e(e + qo[u], pol_e) : 0.f;
                 acc_b = fmaf(wo[u], ev, acc_b);
                 acc_a = fmaf(wo[u], wo[u], acc_a);
             }
@@ -740,10 +787,10 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (qr[r] >= 0) atomicAdd(e + qr[r], -du * wr[r]);
-            for (int64_t base = e0; base < en; base += (int64_t)NP * kU) {
+            for (int base = (int)CAP; base < n; base += NP * kU) {
                 int qo[kU];
                 float wo[kU];
-                load_pair_entries<kU, NP>(pairs, base + j, en, off, half, pol, qo, wo);
+                load_seq_pairs<kU, NP>(pairs, base + j, n, n1, hi, lo, off, half, pol_m, qo, wo);
 #pragma unroll
                 for (int u = 0; u < kU; ++u)
                     if (qo[u] >= 0) atomicAdd(e + qo[u], -du * wo[u]);
@@ -752,6 +799,247 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_pairs_kernel(
             ++n_upd;
         }
         __syncthreads();  // s_item / s_red reused by the next item
+    }
+    flush_counts(stats, n_upd, n_ent, tid);
+}
+
+// ---------------------------------------------------------------------------
+// Bulk-staged CTA kernel: one voxel update per CTA of 8 warps, the update's
+// entry pairs copied into shared memory by the TMA engine
+// (cp.async.bulk, completion on an mbarrier) instead of per-thread loads.
+// The copy of the next item's pairs is issued as soon as a stage is free, so
+// with two stages it runs while the current update gathers, solves and
+// scatters; the column is read from HBM once (gather and scatter both read
+// the stage), and a thread issues all of its ~28 e gathers back to back (one
+// round trip instead of a chain of index-then-gather chunks). Windows longer
+// than the stage stream their tail from global memory twice, as the CTA pairs
+// kernel does. Same per-voxel update as icd_cta_pairs_kernel.
+// ---------------------------------------------------------------------------
+constexpr int kBulkThreads = 256;
+constexpr int kBulkNP = kBulkThreads / 2;        // pairs per row (two threads per pair)
+constexpr int kBulkRows = 28;                    // rows of pairs staged per update
+constexpr int kBulkCap = kBulkNP * kBulkRows;    // 3584 pairs (7168 entries)
+constexpr int kBulkStagePairs = kBulkCap + 2;    // + slack for the 16-byte-aligned start
+constexpr int kBulkHeader = 256;                 // mbarriers and item records
+constexpr uint32_t kBulkChunk = 16384;           // bytes per bulk copy instruction
+constexpr size_t bulk_smem_bytes(int stages) { return kBulkHeader + (size_t)stages * kBulkStagePairs * 8; }
+static_assert((kBulkStagePairs * 8) % 16 == 0, "stage size must keep 16-byte alignment");
+
+struct BulkItem {
+    int64_t b, en;       // pair range of the slice's view window
+    int64_t q;           // voxel index
+    int64_t n_entries;   // matrix entries of the window (statistics)
+    int off, d, ns, valid;  // sinogram offset, stage skew (0/1), staged pairs, item present
+};
+static_assert(2 * sizeof(BulkItem) + 16 <= kBulkHeader, "item records overflow the header");
+
+__device__ __forceinline__ void bulk_mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+__device__ __forceinline__ void bulk_mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool bulk_mbar_try_wait(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n.reg .pred p;\nmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\nselp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Bounded wait (about a second of SM clock); false if it gave up.
+__device__ __forceinline__ bool bulk_mbar_wait(uint32_t bar, uint32_t parity) {
+    const long long t0 = clock64();
+    while (!bulk_mbar_try_wait(bar, parity))
+        if (clock64() - t0 > 2000000000ll) return false;
+    return true;
+}
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Thread 0: take the next work item and start the copy of its pairs into
+// the stage at `dst` (bytes counted on `bar`). Pairs [b0, e1) are copied with
+// b0 = b rounded down and e1 rounded up to even (16-byte boundaries; the pair
+// array has two pairs of padding past its end); the item's first pair sits at
+// stage position d = b - b0.
+__device__ __forceinline__ void bulk_issue(const GParams& P, const uint32_t* __restrict__ order,
+                                           const int64_t* __restrict__ pcolptr, const uint32_t* __restrict__ pvptr,
+                                           const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
+                                           const int32_t* __restrict__ start, unsigned long long* queue,
+                                           BulkItem* it, uint32_t dst, uint32_t bar) {
+    const uint64_t item = atomicAdd(queue, 1ull);
+    if (item >= P.n_items) {
+        it->valid = 0;
+        return;
+    }
+    const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint32_t packed = __ldg(order + item);
+    const uint64_t col = packed / (uint32_t)P.nz;
+    const int k = (int)(packed % (uint32_t)P.nz);
+    const int s = start[k];
+    const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
+    int64_t b = 0, en = 0, ne = 0;
+    if (v1 > v0) {
+        const int64_t cb = pcolptr[col];
+        const uint32_t* vp = pvptr + col * P.nvsm1;
+        b = cb + vp[v0];
+        en = cb + vp[v1];
+        ne = (int64_t)vptr[col * P.nvsm1 + v1] - (int64_t)vptr[col * P.nvsm1 + v0];
+    }
+    const int ns = (int)min(en - b, (int64_t)kBulkCap);
+    const int64_t b0 = b & ~(int64_t)1;
+    const int64_t e1 = (b + ns + 1) & ~(int64_t)1;
+    const uint32_t bytes = ns > 0 ? (uint32_t)((e1 - b0) * 8) : 0u;
+    it->b = b;
+    it->en = en;
+    it->q = (int64_t)col + (int64_t)ncol * k;
+    it->n_entries = ne;
+    it->off = s * P.nch * P.nr;
+    it->d = (int)(b - b0);
+    it->ns = ns;
+    it->valid = 1;
+    // The stage was last read through the generic proxy; order those reads
+    // before the async-proxy writes of the copy.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    bulk_mbar_expect_tx(bar, bytes);
+    const char* src = reinterpret_cast<const char*>(pairs + b0);
+    for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
+}
+
+template <int STAGES>
+__global__ void __launch_bounds__(kBulkThreads, STAGES == 1 ? 4 : 3) icd_bulk_kernel(
+    GParams P, const uint32_t* __restrict__ order, const int64_t* __restrict__ pcolptr,
+    const uint32_t* __restrict__ pvptr, const uint2* __restrict__ pairs, const uint32_t* __restrict__ vptr,
+    const int32_t* __restrict__ start, float* e, float* x, unsigned long long* queue, unsigned long long* stats,
+    unsigned long long* err) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ float s_red[2 * (kBulkThreads / 32) + 1];
+    constexpr int NW = kBulkThreads / 32;
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    const int j = tid >> 1, half = tid & 1;
+    const uint32_t base = (uint32_t)__cvta_generic_to_shared(smem);
+    BulkItem* items = reinterpret_cast<BulkItem*>(smem + 16);
+    auto bar = [&](int s) { return base + 8u * (uint32_t)s; };
+    auto stage_addr = [&](int s) { return base + (uint32_t)kBulkHeader + (uint32_t)s * (uint32_t)(kBulkStagePairs * 8); };
+    const uint64_t pol = l2_normal();
+    unsigned long long n_ent = 0, n_upd = 0;
+    if (tid == 0) {
+        for (int s = 0; s < STAGES; ++s) bulk_mbar_init(bar(s), 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        for (int s = 0; s < STAGES; ++s)
+            bulk_issue(P, order, pcolptr, pvptr, pairs, vptr, start, queue, &items[s], stage_addr(s), bar(s));
+    }
+    uint32_t parity = 0;  // bit s: phase of stage s's barrier to wait for
+    int cur = 0;
+    bool failed = false;
+    for (;;) {
+        __syncthreads();
+        const BulkItem it = items[cur];
+        if (!it.valid) break;
+        const bool ok = bulk_mbar_wait(bar(cur), (parity >> cur) & 1u);
+        if (__syncthreads_or(!ok)) {
+            failed = true;
+            break;
+        }
+        parity ^= 1u << cur;
+        const uint2* stp = reinterpret_cast<const uint2*>(smem + kBulkHeader + (size_t)cur * kBulkStagePairs * 8) + it.d;
+        const int n = (int)(it.en - it.b);
+        float ev[kBulkRows];
+#pragma unroll
+        for (int i = 0; i < kBulkRows; ++i) {
+            const int p = j + kBulkNP * i;
+            float v = 0.f;
+            if (p < it.ns) {
+                const uint2 pr = stp[p];
+                if (!half || (pr.y >> 16)) v = __ldcg(e + ((int)pr.x + it.off + half));
+            }
+            ev[i] = v;
+        }
+        float acc_b = 0.f, acc_a = 0.f;
+#pragma unroll
+        for (int i = 0; i < kBulkRows; ++i) {
+            const int p = j + kBulkNP * i;
+            if (p < it.ns) {
+                const uint32_t wb = stp[p].y;
+                const float wv = half ? half_hi(wb) : half_lo(wb);
+                acc_b = fmaf(wv, ev[i], acc_b);
+                acc_a = fmaf(wv, wv, acc_a);
+            }
+        }
+        for (int b2 = it.ns; b2 < n; b2 += kBulkNP * kU) {
+            int qo[kU];
+            float wo[kU];
+            load_pair_entries<kU, kBulkNP>(pairs, it.b + b2 + j, it.en, it.off, half, pol, qo, wo);
+#pragma unroll
+            for (int u = 0; u < kU; ++u) {
+                const float evu = qo[u] >= 0 ? __ldcg(e + qo[u]) : 0.f;
+                acc_b = fmaf(wo[u], evu, acc_b);
+                acc_a = fmaf(wo[u], wo[u], acc_a);
+            }
+        }
+        acc_b = warp_sum(acc_b);
+        acc_a = warp_sum(acc_a);
+        if (lane == 0) {
+            s_red[wid] = acc_b;
+            s_red[NW + wid] = acc_a;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            double beta = 0.0, alpha = 0.0;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) {
+                beta += (double)s_red[i];
+                alpha += (double)s_red[NW + i];
+            }
+            const double xq = (double)__ldcg(x + it.q);
+            double upd = penalty_step(P, x, it.q, xq, alpha, beta, lane) * P.relax;
+            if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
+            if (lane == 0) {
+                x[it.q] = (float)(xq + upd);
+                s_red[2 * NW] = (float)upd;
+            }
+        }
+        __syncthreads();
+        const float du = s_red[2 * NW];
+        if (du != 0.f) {
+#pragma unroll
+            for (int i = 0; i < kBulkRows; ++i) {
+                const int p = j + kBulkNP * i;
+                if (p < it.ns) {
+                    const uint2 pr = stp[p];
+                    if (!half || (pr.y >> 16))
+                        atomicAdd(e + ((int)pr.x + it.off + half), -du * (half ? half_hi(pr.y) : half_lo(pr.y)));
+                }
+            }
+            for (int b2 = it.ns; b2 < n; b2 += kBulkNP * kU) {
+                int qo[kU];
+                float wo[kU];
+                load_pair_entries<kU, kBulkNP>(pairs, it.b + b2 + j, it.en, it.off, half, pol, qo, wo);
+#pragma unroll
+                for (int u = 0; u < kU; ++u)
+                    if (qo[u] >= 0) atomicAdd(e + qo[u], -du * wo[u]);
+            }
+            n_ent += (unsigned long long)it.n_entries;
+            ++n_upd;
+        }
+        __syncthreads();  // the stage, the item record and s_red are free
+        if (tid == 0)
+            bulk_issue(P, order, pcolptr, pvptr, pairs, vptr, start, queue, &items[cur], stage_addr(cur), bar(cur));
+        cur = cur + 1 == STAGES ? 0 : cur + 1;
+    }
+    if (failed) {
+        // A copy that never completed: record it, then wait (bounded) for any
+        // copy still writing this CTA's shared memory before exiting.
+        if (tid == 0) {
+            atomicExch(err, 1ull);
+            for (int c = 0; c < STAGES; ++c)
+                if (items[c].valid) bulk_mbar_wait(bar(c), (parity >> c) & 1u);
+        }
+        __syncthreads();
     }
     flush_counts(stats, n_upd, n_ent, tid);
 }
@@ -985,9 +1273,14 @@ __global__ void __launch_bounds__(32 * NW, 1) icd_staged_kernel(GParams P, const
 // from the gather to the scatter, so the matrix column is read from memory
 // once per update and the reductions hit e's lines while they are still in
 // L2; with one item per CTA, one to a few updates per SM are in flight.
-// Entries beyond 32 * WPV * R (rare) are streamed twice.
+// Entries beyond 32 * WPV * R (rare) are streamed twice. With
+// P.stack_align the sweep starts at the slice stack's common data view and
+// wraps around (as in process_item), so the stack's members, consecutive in
+// the visiting order, touch each shared sinogram sector within microseconds
+// of one another; with P.l2_hints the matrix loads (read once) are marked
+// evict-first and the e gathers evict-last.
 template <class WT, int WPV, int R>
-__global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint32_t* __restrict__ order,
+__global__ void __launch_bounds__(32 * WPV, 16 / WPV) icd_cta_kernel(GParams P, const uint32_t* __restrict__ order,
                                                         const int64_t* __restrict__ colptr,
                                                         const uint32_t* __restrict__ vptr,
                                                         const int32_t* __restrict__ idx, const WT* __restrict__ w,
@@ -1000,6 +1293,8 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
     __shared__ float s_red[2 * WPV + 1];
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     const uint64_t ncol = (uint64_t)P.nx * P.ny;
+    const uint64_t pol_m = P.l2_hints ? l2_drop() : l2_normal();
+    const uint64_t pol_e = P.l2_hints ? l2_keep() : l2_normal();
     for (;;) {
         if (tid == 0) s_item = atomicAdd(queue, 1ull);
         __syncthreads();
@@ -1011,23 +1306,29 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
         const int64_t q = (int64_t)col + (int64_t)ncol * k;
         const int s = start[k];
         const int v0 = max(0, -s), v1 = min(P.nvsm, P.readings - s);
-        int64_t b = 0, en = 0;
+        int64_t b = 0, en = 0, mid = 0;
         if (v1 > v0) {
             const int64_t cb = colptr[col];
             const uint32_t* vp = vptr + col * P.nvsm1;
             b = cb + vp[v0];
             en = cb + vp[v1];
+            mid = P.stack_align ? cb + vp[stack_start_view(P, start, k, s, v0, v1)] : b;
         }
         const int off = s * P.nch * P.nr;
-        const int64_t e0 = min(en, b + CAP);
+        // Sweep position p -> entry p + hi for p < n1 ([mid, en)), else p + lo
+        // ([b, mid)).
+        const int n = (int)(en - b), n1 = (int)(en - mid);
+        const int64_t hi = mid, lo = b - n1;
+        const int nreg = min(n, (int)CAP);
         int qr[R];
         float wr[R];
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const int64_t m = b + tid + (int64_t)NT * r;
-            if (m < e0) {
-                qr[r] = __ldg(idx + m) + off;
-                wr[r] = ldw(w, m);
+            const int p = tid + NT * r;
+            if (p < nreg) {
+                const int64_t m = (p < n1 ? hi : lo) + p;
+                qr[r] = ld_idx(idx + m, pol_m) + off;
+                wr[r] = ldw_hint(w, m, pol_m);
             } else {
                 qr[r] = -1;
                 wr[r] = 0.f;
@@ -1036,22 +1337,27 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
         float acc_b = 0.f, acc_a = 0.f;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
-            const float ev = qr[r] >= 0 ? __ldcg(e + qr[r]) : 0.f;
+            const float ev = qr[r] >= 0 ? ld_e(e + qr[r], pol_e) : 0.f;
             acc_b = fmaf(wr[r], ev, acc_b);
             acc_a = fmaf(wr[r], wr[r], acc_a);
         }
-        for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+        for (int base = (int)CAP; base < n; base += NT * kU) {
             int qo[kU];
             float wo[kU];
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const int64_t m = base + tid + (int64_t)NT * u;
-                qo[u] = m < en ? __ldg(idx + m) + off : -1;
-                wo[u] = m < en ? ldw(w, m) : 0.f;
+                const int p = base + tid + NT * u;
+                qo[u] = -1;
+                wo[u] = 0.f;
+                if (p < n) {
+                    const int64_t m = (p < n1 ? hi : lo) + p;
+                    qo[u] = ld_idx(idx + m, pol_m) + off;
+                    wo[u] = ldw_hint(w, m, pol_m);
+                }
             }
 #pragma unroll
             for (int u = 0; u < kU; ++u) {
-                const float ev = qo[u] >= 0 ? __ldcg(e + qo[u]) : 0.f;
+                const float ev = qo[u] >= 0 ? ld_e(e + qo[u], pol_e) : 0.f;
                 acc_b = fmaf(wo[u], ev, acc_b);
                 acc_a = fmaf(wo[u], wo[u], acc_a);
             }
@@ -1084,11 +1390,14 @@ __global__ void __launch_bounds__(32 * WPV) icd_cta_kernel(GParams P, const uint
 #pragma unroll
             for (int r = 0; r < R; ++r)
                 if (qr[r] >= 0) atomicAdd(e + qr[r], -du * wr[r]);
-            for (int64_t base = e0; base < en; base += (int64_t)NT * kU) {
+            for (int base = (int)CAP; base < n; base += NT * kU) {
 #pragma unroll
                 for (int u = 0; u < kU; ++u) {
-                    const int64_t m = base + tid + (int64_t)NT * u;
-                    if (m < en) atomicAdd(e + (__ldg(idx + m) + off), -du * ldw(w, m));
+                    const int p = base + tid + NT * u;
+                    if (p < n) {
+                        const int64_t m = (p < n1 ? hi : lo) + p;
+                        atomicAdd(e + (ld_idx(idx + m, pol_m) + off), -du * ldw_hint(w, m, pol_m));
+                    }
                 }
             }
             n_ent += (unsigned long long)(en - b);
@@ -1255,6 +1564,7 @@ __global__ void __launch_bounds__(256) count_entries_kernel(GParams P, const uin
 GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_opts& o) {
     const ctbb_geom_c& g = rc->geom;
     GParams P;
+    memset(&P, 0, sizeof(P));  // compared bytewise as part of the graph key
     P.nx = (int)g.num_voxels_x;
     P.ny = (int)g.num_voxels_y;
     P.nz = (int)g.num_voxels_z;
@@ -1275,6 +1585,8 @@ GParams make_params(const ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_icd_op
     P.vx = g.voxel_size_x;
     P.vy = g.voxel_size_y;
     P.fov_limit = (g.acquisition_fov / 2.0) * (g.acquisition_fov / 2.0);
+    P.stack_align = o.stack_align == 1 ? 1 : 0;
+    P.l2_hints = o.l2_hints == 1 ? 1 : 0;
     return P;
 }
 
@@ -1309,10 +1621,14 @@ uint64_t requested_items(const ctbb_recon* rc, const ctbb_icd_opts& o) {
     // put a large share of the voxels on each ray in flight at once, and the
     // edge-preserving iteration then oscillates.
     const int coupling = default_warps_in_flight(rc);
+    // The bulk-staged kernel keeps four CTAs (one stage) or three (two
+    // stages) of 8 warps per SM.
+    const int bulk = rc->ctx->sm_count * (o.stage_column == 4 ? 4 : 3) * (kBulkThreads / 32);
     const int W = o.warps_in_flight > 0 ? o.warps_in_flight
+                  : o.stage_column >= 4 ? std::min(bulk, coupling)
                   : o.stage_column == 3 ? std::min(lockstep, coupling)
                   : (o.stage_column ? std::min(staged, coupling) : coupling);
-    const int wpv = o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
+    const int wpv = o.stage_column >= 4 ? kBulkThreads / 32 : o.warps_per_voxel > 1 ? o.warps_per_voxel : 1;
     return std::max<uint64_t>(1, (uint64_t)(W / wpv));
 }
 
@@ -1603,9 +1919,10 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     if (wpv != 1 && wpv != 4 && wpv != 8)
         return fail(CTBB_ERR_INVALID_ARG, "warps_per_voxel must be 1, 4 or 8 (got %d)", wpv);
     const int stage = o.stage_column;
-    if (stage < 0 || stage > 3)
-        return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0, 1, 2 or 3 (got %d)", stage);
-    if (stage && wpv != 1) return fail(CTBB_ERR_INVALID_ARG, "stage_column needs one warp per voxel update");
+    if (stage < 0 || stage > 5)
+        return fail(CTBB_ERR_INVALID_ARG, "stage_column must be 0 to 5 (got %d)", stage);
+    if (stage >= 1 && stage <= 3 && wpv != 1)
+        return fail(CTBB_ERR_INVALID_ARG, "stage_column 1-3 needs one warp per voxel update");
     const uint32_t* stacks = prio ? rc->d_prio_stacks : rc->d_stacks;
     const uint64_t n_stacks = prio ? rc->n_prio_stacks : rc->n_stacks;
     if (stage == 3 && !stacks) return fail(CTBB_ERR_INVALID_ARG, "visiting order has no stack table");
@@ -1618,9 +1935,13 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     const bool h = wsel == CTBB_SSM_FP16;
     // Entry pairs for the CTA-per-update kernels with FP16 weights (built
     // here, outside any stream capture, on first use).
-    const bool want_pairs = h && o.entry_pairs == 0 && (wpv > 1 || stage == 0);
+    const bool want_pairs = h && (stage >= 4 || (o.entry_pairs == 0 && (wpv > 1 || stage == 0)));
     if (want_pairs) CTBB_TRY(ssm_build_pairs(const_cast<ctbb_ssm*>(ssm)));
     const bool pairs = want_pairs && ssm->d_pairs;
+    if (stage >= 4 && !pairs)
+        return fail(CTBB_ERR_INVALID_ARG,
+                    "stage_column 4/5 reads entry pairs: needs FP16 weights and a matrix whose detector-row runs "
+                    "pair up (no z flying focal spot)");
     const int64_t* cp = ssm->d_colptr;
     const uint32_t* vp = ssm->d_vptr;
     const int32_t* ix = ssm->d_idx;
@@ -1628,7 +1949,32 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     // One iteration: reset the work queue and the scatter counters, then the
     // persistent kernel (prepare: only the launch attributes, no work).
     auto issue = [&](cudaStream_t s, bool prepare) -> ctbb_status {
-        if (!prepare) CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 4 * sizeof(unsigned long long), s));
+        if (!prepare) CTBB_CUDA(cudaMemsetAsync(ctx->d_queue, 0, 5 * sizeof(unsigned long long), s));
+        if (stage >= 4) {
+            // One update per CTA of 8 warps; 4: one pair stage, 5: two.
+            const int stages = stage == 4 ? 1 : 2;
+            const size_t smem = bulk_smem_bytes(stages);
+            if (prepare) {
+                if (stages == 1)
+                    CTBB_CUDA(cudaFuncSetAttribute(icd_bulk_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem));
+                else
+                    CTBB_CUDA(cudaFuncSetAttribute(icd_bulk_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                   (int)smem));
+                return CTBB_OK;
+            }
+            const int blocks = (int)std::max<uint64_t>(1, in_flight);
+            if (stages == 1)
+                icd_bulk_kernel<1><<<blocks, kBulkThreads, smem, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                      ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                      rc->d_x32, ctx->d_queue, stats, stats + 2);
+            else
+                icd_bulk_kernel<2><<<blocks, kBulkThreads, smem, s>>>(P, order, ssm->d_pcolptr, ssm->d_pvptr,
+                                                                      ssm->d_pairs, vp, rc->d_start, rc->d_e32,
+                                                                      rc->d_x32, ctx->d_queue, stats, stats + 2);
+            CTBB_CUDA(cudaGetLastError());
+            return CTBB_OK;
+        }
         if (stage == 3) {
             if (prepare) return CTBB_OK;
             // One CTA (kStack warps) per stack: at most in_flight / kStack
@@ -1791,11 +2137,13 @@ ctbb_status launch_icd_grouped(ctbb_recon* rc, const ctbb_ssm* ssm, const ctbb_i
     cudaEventElapsedTime(ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    if (scattered) {
-        unsigned long long h2[2] = {0, 0};
-        CTBB_CUDA(cudaMemcpyAsync(h2, stats, sizeof(h2), cudaMemcpyDeviceToHost, st));
+    if (scattered || stage >= 4) {
+        unsigned long long h3[3] = {0, 0, 0};
+        CTBB_CUDA(cudaMemcpyAsync(h3, stats, sizeof(h3), cudaMemcpyDeviceToHost, st));
         CTBB_CUDA(cudaStreamSynchronize(st));
-        *scattered = (double)h2[1];
+        if (scattered) *scattered = (double)h3[1];
+        if (h3[2]) return fail(CTBB_ERR_CUDA, "bulk-staged ICD kernel: a matrix copy into shared memory did not "
+                                              "complete within its wait limit");
     }
     return CTBB_OK;
 }

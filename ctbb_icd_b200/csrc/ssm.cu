@@ -481,7 +481,10 @@ ctbb_status ssm_build_pairs(ctbb_ssm* s) {
         CTBB_CUDA(cudaMemcpyAsync(&np, s->d_pcolptr + s->ncol, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
         CTBB_CUDA(cudaStreamSynchronize(st));
         s->npairs = (uint64_t)np;
-        CTBB_CUDA(cudaMalloc(&s->d_pairs, std::max<uint64_t>(1, s->npairs) * sizeof(uint2)));
+        // Two pairs of padding: the bulk-staged ICD kernel copies whole 16-byte
+        // units and may read one pair past the last.
+        CTBB_CUDA(cudaMalloc(&s->d_pairs, (s->npairs + 2) * sizeof(uint2)));
+        CTBB_CUDA(cudaMemsetAsync(s->d_pairs + s->npairs, 0, 2 * sizeof(uint2), st));
         ssm_pairs_kernel<true><<<grid, 256, 0, st>>>(s->ncol, (int)s->nvsm, s->d_colptr, s->d_vptr, s->d_idx,
                                                      s->d_w16, nullptr, s->d_pcolptr, s->d_pvptr, s->d_pairs);
         CTBB_CUDA(cudaGetLastError());

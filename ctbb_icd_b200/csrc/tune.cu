@@ -87,6 +87,12 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     if (o.weights == CTBB_SSM_FP16) cands.push_back({4, 4 * sms * 4, 8, 0, 0, -1});
     cands.push_back({4, 8 * sms * 4, 8, 0, 0, 0});
     cands.push_back({8, 4 * sms * 8, 8, 0, 0, 0});
+    // One update per CTA of 8 warps with the entry pairs bulk-copied into
+    // shared memory: one stage (four CTAs per SM) or two (three per SM).
+    if (o.weights == CTBB_SSM_FP16) {
+        cands.push_back({8, 4 * sms * 8, 8, 0, 4, 0});
+        cands.push_back({8, 3 * sms * 8, 8, 0, 5, 0});
+    }
     struct Trial {
         int wpv, w, epl, t, stage, pairs;
         double ms, cost, score;

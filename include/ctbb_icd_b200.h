@@ -299,7 +299,13 @@ typedef struct ctbb_icd_opts {
                                  slices at one physical cell) as one CTA whose
                                  warps sweep the stack's data views in lockstep,
                                  so the sinogram sectors they share are fetched
-                                 from HBM once                                     */
+                                 from HBM once; 4 and 5 (FP16 weights, entry
+                                 pairs) run one update per CTA of 8 warps whose
+                                 entry pairs the TMA engine copies into shared
+                                 memory (one bulk copy per update, read by both
+                                 gather and scatter), with one stage (4) or two
+                                 (5: the next update's copy overlaps the current
+                                 update); warps_in_flight counts 8 per update     */
     int32_t entry_pairs;      /* grouped, FP16 weights, one warp per voxel (streamed,
                                  stage_column 0; entries_per_lane then counts pairs)
                                  or 4 or 8 warps per voxel: 0
@@ -309,6 +315,17 @@ typedef struct ctbb_icd_opts {
                                  matrix on first use and kept where pairs hold
                                  4/3 entries or more on average); -1 reads single
                                  entries (4-byte index + 2-byte weight)           */
+    int32_t stack_align;      /* grouped, 4 or 8 warps per voxel: 1 starts each
+                                 update's sweep of its view window at the data view
+                                 where its slice stack's last member's window
+                                 begins, wrapping around to the window start, so
+                                 the stack's members (consecutive in the visiting
+                                 order) read and update the sinogram sectors they
+                                 share at about the same time; 0 sweeps each window
+                                 from its start                                   */
+    int32_t l2_hints;         /* grouped, 4 or 8 warps per voxel: 1 marks the matrix
+                                 loads (read once per update) evict-first and the
+                                 e gathers evict-last in L2; 0 leaves both normal */
 } ctbb_icd_opts;
 
 /*

@@ -200,7 +200,7 @@ def converged_cfg1_small(ctx, tmp_path_factory):
 @pytest.mark.parametrize("weights,wpv,stage,pairs", [
     (C.SSM_FP32, 1, 0, 0), (C.SSM_FP16, 1, 0, 0), (C.SSM_FP16, 1, 0, -1), (C.SSM_FP32, 8, 0, 0), (C.SSM_FP16, 4, 0, 0),
     (C.SSM_FP16, 8, 0, 0), (C.SSM_FP16, 4, 0, -1), (C.SSM_FP16, 1, 1, 0), (C.SSM_FP32, 1, 2, 0),
-    (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0)])
+    (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0), (C.SSM_FP16, 8, 4, 0), (C.SSM_FP16, 8, 5, 0)])
 def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage, pairs):
     """FP16 with the streamed (one warp) or 4/8-warp kernels reads the
     matrix as entry pairs (pairs 0) or as single entries (pairs -1)."""
@@ -242,6 +242,28 @@ def test_entry_pairs_match_single_entries(ctx, converged_cfg1_small, wpv):
     # runs of two detector rows make most pairs (a lone entry takes a pair too)
     info = ssm.info()
     assert info.nnz / 2 <= info.n_pairs <= 0.75 * info.nnz, (info.n_pairs, info.nnz)
+
+
+@pytest.mark.parametrize("stage", [4, 5])
+@pytest.mark.parametrize("case", ["cfg1_small", "small_ffs"])
+def test_bulk_staged_kernel_matches_cta_pairs(ctx, converged_cfg1_small, converged_small_ffs, case, stage):
+    """One update in flight: the kernel whose entry pairs arrive in shared
+    memory by bulk copy gives the iterates of the CTA kernel that loads the
+    same pairs into registers, up to the order of the FP32 partial sums.
+    cfg1_small's windows are longer than the shared-memory stage (3584
+    pairs), so their tails take the streamed path as well."""
+    rp, data, ssm, _, _ = converged_cfg1_small if case == "cfg1_small" else converged_small_ffs
+    out = {}
+    for st in (0, stage):
+        rc = C.Recon(rp, data.slice_indices, ctx)
+        rc.set_raw(data.raw)
+        rc.set_volume(ssm, None)
+        rc.iterate(ssm, 2, C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP16, warps_per_voxel=8,
+                                      warps_in_flight=8, stage_column=st))
+        out[st] = rc.volume_f64()
+        rc.free()
+    a, b = out[stage], out[0]
+    assert np.linalg.norm(a - b) <= 1e-5 * np.linalg.norm(b), np.linalg.norm(a - b) / np.linalg.norm(b)
 
 
 def test_batch_of_uneven_scans_converges(ctx, converged_cfg1_small, tmp_path):
@@ -306,7 +328,7 @@ def converged_small_ffs(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1), (C.SSM_FP16, 3)])
+@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1), (C.SSM_FP16, 3), (C.SSM_FP16, 5)])
 def test_grouped_edge_preserving_reaches_converged_cost(ctx, converged_small_ffs, weights, stage):
     rp, data, ssm, x_ref, cost_ref = converged_small_ffs
     rc = C.Recon(rp, data.slice_indices, ctx)
