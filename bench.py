@@ -234,10 +234,10 @@ def run_ours(args, rank, world, dist):
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
         kernel = ("icd_bulk_kernel" if opts.stage_column >= 4 else
-                  "icd_lockstep_kernel" if opts.stage_column == 3 else
-                  "icd_staged_kernel" if opts.stage_column else
-                  "icd_grouped_pairs_kernel" if uses_pairs else "icd_grouped_kernel") \
-            if opts.warps_per_voxel <= 1 else ("icd_cta_pairs_kernel" if uses_pairs else "icd_cta_kernel")
+                  ("icd_lockstep_kernel" if opts.stage_column == 3 else
+                   "icd_staged_kernel" if opts.stage_column else
+                   "icd_grouped_pairs_kernel" if uses_pairs else "icd_grouped_kernel")
+                  if opts.warps_per_voxel <= 1 else ("icd_cta_pairs_kernel" if uses_pairs else "icd_cta_kernel"))
         traffic = read_traffic(kernel)
         out = {
             "metric": "voxel-updates/s",
@@ -286,6 +286,8 @@ def run_ours(args, rank, world, dist):
             out["cpu_baseline"] = {k: cb.get(k) for k in ("value", "unit", "cores", "kind", "sample")}
     rc.free()
     ssm.free()
+    if out is not None and args.ttt and world == 1:
+        out["time_to_tolerance"] = time_to_tolerance_sample(ctx, opts)
     ctx.close()
     return out
 
@@ -617,6 +619,68 @@ def read_traffic(kernel: str = "icd_grouped_kernel"):
     return None
 
 
+TTT_LADDER = (1000.0, 500.0, 200.0, 100.0, 50.0, 25.0, 10.0, 5.0, 2.0, 1.0, 0.5)
+
+
+def time_to_tolerance_sample(ctx, tuned, seed=900, ref_iter=300, max_iter=80):
+    """The second half of the benchmark metric on a bounded sample: wall time
+    of plain grouped ICD and of the learned warm start to each RMSE tolerance
+    (HU, inside the object support, interior slices) against a reference
+    image, on a held-out scan of the network's training grid (cfg2's scanner,
+    flying focal spot and penalty at 256 x 256 x 32, 1.17 mm voxels). The
+    reference is the learned start followed by `ref_iter` iterations; both
+    arms start from the zero image and run at most `max_iter` iterations with
+    the main run's autotuned kernel settings. Reports each tolerance's times,
+    the tightest tolerance both arms reach, and how far the reference itself
+    still moved over its last ten iterations."""
+    import ctbb_icd_b200 as C
+    from ctbb_icd_b200 import learned as L
+
+    t0 = time.time()
+    net = L.WarmStartNet.load(ctx, L.WEIGHTS_PATH)
+    scan = L.make_scan(ctx, L.TRAIN_WORKLOAD, seed, weights=C.SSM_FP16)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP16, warps_per_voxel=tuned.warps_per_voxel,
+                      warps_in_flight=tuned.warps_in_flight, entries_per_lane=tuned.entries_per_lane,
+                      stage_column=tuned.stage_column, entry_pairs=tuned.entry_pairs)
+    scan.rc.set_volume(scan.ssm, None)
+    scan.rc.iterate(scan.ssm, net.n_early, net.early_opts(scan.rc, opts))
+    scan.rc.warm_start(scan.ssm, net, scan.tables.tube_angles)
+    done = 0
+    while done < ref_iter - 10:
+        n = min(50, ref_iter - 10 - done)
+        scan.rc.iterate(scan.ssm, n, opts)
+        scan.rc.refresh_residual(scan.ssm)
+        done += n
+    x_tail = scan.rc.volume()
+    scan.rc.iterate(scan.ssm, 10, opts)
+    scan.rc.refresh_residual(scan.ssm)
+    x_ref = scan.rc.volume()
+    motion = scan.error_hu(x_tail, x_ref)
+    plain = L.time_to_tolerance(scan, x_ref, opts, tol_hu=min(TTT_LADDER), max_iter=max_iter, tols=TTT_LADDER)
+    learned = L.time_to_tolerance(scan, x_ref, opts, tol_hu=min(TTT_LADDER), max_iter=max_iter, net=net,
+                                  n_early=net.n_early, tols=TTT_LADDER)
+    rows, tightest = [], None
+    for tol in TTT_LADDER:
+        a, b = plain["seconds_to"][str(tol)], learned["seconds_to"][str(tol)]
+        rows.append([tol, None if a is None else round(a, 3), None if b is None else round(b, 3)])
+        if a is not None and b is not None:
+            tightest = (tol, a, b)
+    scan.rc.free()
+    scan.ssm.free()
+    return {
+        "workload": f"held-out seed {seed} of the warm-start training grid ({L.TRAIN_WORKLOAD}: "
+                    "256x256x32 at 1.17 mm, cfg2 scanner, in-plane FFS, edge-preserving)",
+        "reference": f"learned start + {ref_iter} iterations; moved {motion:.3f} HU RMSE over its last 10",
+        "fields": ["hu", "plain_s", "learned_s"], "seconds_to_hu": rows,
+        "tightest_both": None if tightest is None else
+        {"hu": tightest[0], "plain_s": round(tightest[1], 3), "learned_s": round(tightest[2], 3),
+         "learned_over_plain": round(tightest[2] / tightest[1], 3) if tightest[1] > 0 else None},
+        "final_hu": {"plain": round(plain["trace"][-1][2], 3), "learned": round(learned["trace"][-1][2], 3),
+                     "iterations": max_iter},
+        "wall_s": round(time.time() - t0, 1),
+    }
+
+
 # --------------------------------------------------------------------------
 # Reference arm / CPU baseline
 # --------------------------------------------------------------------------
@@ -777,6 +841,8 @@ def main():
     ap.add_argument("--no-e2e", dest="e2e", action="store_false")
     ap.add_argument("--e2e-steps", type=int, default=1, help="timed drop-in calls (each runs --steps iterations)")
     ap.add_argument("--no-cpu-baseline", dest="cpu_baseline", action="store_false")
+    ap.add_argument("--no-ttt", dest="ttt", action="store_false",
+                    help="skip the time-to-tolerance sample (plain vs learned warm start)")
     ap.add_argument("--no-clocks", dest="clocks", action="store_false", help="skip nvidia-smi clock sampling")
     ap.add_argument("--own-stream", action="store_true", help="run on the library's own stream")
     ap.add_argument("--stage", choices=["icd", "ssm", "rotate", "cnn", "batch"], default="icd",

@@ -353,9 +353,10 @@ __device__ __forceinline__ double penalty_solve(int penalty, double lam, double 
     double step_old = hi - lo, step = step_old;
     for (int it = 0; it < 64; ++it) {
         const double t = c - diff;
-        const double den = del + fabs(t);
-        const double f = 2.0 * alpha * c - 2.0 * beta + lam * sum8(wn * t / den);
-        const double fp = 2.0 * alpha + lam * sum8(wn * del / (den * den));
+        const double r = 1.0 / (del + fabs(t));  // one division per lane and iteration
+        const double wr = wn * r;
+        const double f = 2.0 * alpha * c - 2.0 * beta + lam * sum8(wr * t);
+        const double fp = 2.0 * alpha + lam * sum8(wr * del * r);
         if (f > 0.0)
             hi = c;
         else
@@ -374,6 +375,22 @@ __device__ __forceinline__ double penalty_solve(int penalty, double lam, double 
 // Penalised 1-D update of voxel q by one warp (lanes 0-7 hold the 8 in-plane
 // neighbours of penalties.cpp:41-52 / 67-74, flat-index offsets, a neighbour
 // outside [0, nvox) dropped).
+// The neighbour of voxel q that lane 0-7 holds, as loaded from x (lane
+// >= 8 or outside [0, nvox): *w = 0). Loaded before the update's gather so
+// the value is in a register when the penalty solve starts.
+__device__ __forceinline__ float neighbour_value(const GParams& P, const float* x, int64_t q, int lane, double* w) {
+    *w = 0.0;
+    if (lane >= 8) return 0.f;
+    const int64_t nx = P.nx;
+    const int64_t nvox = (int64_t)P.nx * P.ny * P.nz;
+    const int64_t dr = lane < 3 ? -1 : (lane < 5 ? 0 : 1);
+    const int64_t dc = lane < 3 ? lane - 1 : (lane < 5 ? 2 * lane - 7 : lane - 6);
+    const int64_t n = q + dr * nx + dc;
+    if (n < 0 || n >= nvox) return 0.f;
+    *w = neighbour_weight(lane);
+    return __ldcg(x + n);
+}
+
 __device__ __forceinline__ double penalty_step(const GParams& P, const float* x, int64_t q, double xq, double alpha,
                                                double beta, int lane) {
     const int64_t nx = P.nx;
@@ -948,6 +965,14 @@ __global__ void __launch_bounds__(kBulkThreads, STAGES == 1 ? 4 : 3) icd_bulk_ke
         parity ^= 1u << cur;
         const uint2* stp = reinterpret_cast<const uint2*>(smem + kBulkHeader + (size_t)cur * kBulkStagePairs * 8) + it.d;
         const int n = (int)(it.en - it.b);
+        // Warp 0 loads the voxel and its in-plane neighbours now; they are in
+        // registers when the penalty solve starts after the gather.
+        double wn = 0.0;
+        float xn = 0.f, xqf = 0.f;
+        if (wid == 0) {
+            xn = neighbour_value(P, x, it.q, lane, &wn);
+            xqf = __ldcg(x + it.q);
+        }
         float ev[kBulkRows];
 #pragma unroll
         for (int i = 0; i < kBulkRows; ++i) {
@@ -995,8 +1020,9 @@ __global__ void __launch_bounds__(kBulkThreads, STAGES == 1 ? 4 : 3) icd_bulk_ke
                 beta += (double)s_red[i];
                 alpha += (double)s_red[NW + i];
             }
-            const double xq = (double)__ldcg(x + it.q);
-            double upd = penalty_step(P, x, it.q, xq, alpha, beta, lane) * P.relax;
+            const double xq = (double)xqf;
+            const double diff = wn != 0.0 ? (double)xn - xq : 0.0;
+            double upd = penalty_solve(P.penalty, P.lambda, P.delta, alpha, beta, diff, wn) * P.relax;
             if (upd + xq < 0.0) upd = -xq;  // icd_iteration.cpp:233-234
             if (lane == 0) {
                 x[it.q] = (float)(xq + upd);
