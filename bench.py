@@ -233,7 +233,8 @@ def run_ours(args, rank, world, dist):
         peak, peak_kind = measured_peak()
         achieved = b_iter / (kernel_ms_per_launch / 1e3) / 1e9
         value = world * nvox * args.steps / (t_max / 1e3)
-        kernel = ("icd_bulk_kernel" if opts.stage_column >= 4 else
+        kernel = ("icd_bulk_pipe_kernel" if opts.stage_column == 6 else
+                  "icd_bulk_kernel" if opts.stage_column >= 4 else
                   ("icd_lockstep_kernel" if opts.stage_column == 3 else
                    "icd_staged_kernel" if opts.stage_column else
                    "icd_grouped_pairs_kernel" if uses_pairs else "icd_grouped_kernel")
@@ -862,7 +863,9 @@ def main():
                          "evict-last")
     ap.add_argument("--stage-column", type=int, default=-1,
                     help="with --no-autotune: 0 streams each column twice, 1/2 stage it in shared memory, "
-                         "3 sweeps each slice stack in lockstep in one CTA")
+                         "3 sweeps each slice stack in lockstep in one CTA, 4/5 bulk-copy each update's entry "
+                         "pairs into one/two shared-memory stages, 6 the one-stage form with the next item claimed "
+                         "ahead")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -92,6 +92,9 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     if (o.weights == CTBB_SSM_FP16) {
         cands.push_back({8, 4 * sms * 8, 8, 0, 4, 0});
         cands.push_back({8, 3 * sms * 8, 8, 0, 5, 0});
+        // The one-stage kernel with the next item claimed during the
+        // current update's penalty solve, four CTAs per SM.
+        cands.push_back({8, 4 * sms * 8, 8, 0, 6, 0});
     }
     struct Trial {
         int wpv, w, epl, t, stage, pairs;
@@ -112,9 +115,11 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
             const int t_auto = lattice_spacing(rc, c);
             c.lattice = cd.half ? std::max(4, t_auto / 2) : t_auto;
             if (cd.half && c.lattice == t_auto) continue;
-            const uint64_t items = std::min<uint64_t>(
-                requested_items(rc, c), max_items_in_flight(rc->n_order ? rc->n_order : rc->nvox,
-                                                            (int)rc->geom.num_voxels_z, c.lattice));
+            const uint64_t bound = max_items_in_flight(rc->n_order ? rc->n_order : rc->nvox,
+                                                       (int)rc->geom.num_voxels_z, c.lattice);
+            // The claim-ahead bulk kernel holds two claimed items per CTA.
+            const uint64_t items = std::max<uint64_t>(
+                1, std::min<uint64_t>(requested_items(rc, c), cd.stage == 6 ? bound / 2 : bound));
             c.warps_in_flight = (int)(items * (uint64_t)cd.wpv);
             bool seen = false;
             for (const Trial& tr : trials)

@@ -305,7 +305,12 @@ typedef struct ctbb_icd_opts {
                                  memory (one bulk copy per update, read by both
                                  gather and scatter), with one stage (4) or two
                                  (5: the next update's copy overlaps the current
-                                 update); warps_in_flight counts 8 per update     */
+                                 update); 6 is the one-stage form with the next
+                                 item claimed (work queue, visiting order,
+                                 column offsets) during the current update's
+                                 penalty solve (a CTA holds two claimed items,
+                                 so half the order's bound in flight);
+                                 warps_in_flight counts 8 per update              */
     int32_t entry_pairs;      /* grouped, FP16 weights, one warp per voxel (streamed,
                                  stage_column 0; entries_per_lane then counts pairs)
                                  or 4 or 8 warps per voxel: 0
@@ -485,7 +490,8 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
  * coupling-bound default of warps in flight, with 8 or 16 entries per lane
  * in flight and the default tile edge for that concurrency (half of it too
  * at the default); 4 warps per voxel with four or eight updates per SM and
- * 8 warps per voxel with four (these read entry pairs with FP16 weights).
+ * 8 warps per voxel with four (these read entry pairs with FP16 weights);
+ * with FP16 weights, the bulk-staged kernels (stage_column 4, 5 and 6).
  * Every launch keeps at most one cell rank of the visiting order (about
  * n / T^2 updates for tile edge T) in flight, so no two in-plane neighbours
  * of a slice are ever updated together; trials report the effective warps

@@ -200,7 +200,8 @@ def converged_cfg1_small(ctx, tmp_path_factory):
 @pytest.mark.parametrize("weights,wpv,stage,pairs", [
     (C.SSM_FP32, 1, 0, 0), (C.SSM_FP16, 1, 0, 0), (C.SSM_FP16, 1, 0, -1), (C.SSM_FP32, 8, 0, 0), (C.SSM_FP16, 4, 0, 0),
     (C.SSM_FP16, 8, 0, 0), (C.SSM_FP16, 4, 0, -1), (C.SSM_FP16, 1, 1, 0), (C.SSM_FP32, 1, 2, 0),
-    (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0), (C.SSM_FP16, 8, 4, 0), (C.SSM_FP16, 8, 5, 0)])
+    (C.SSM_FP16, 1, 3, 0), (C.SSM_FP32, 1, 3, 0), (C.SSM_FP16, 8, 4, 0), (C.SSM_FP16, 8, 5, 0),
+    (C.SSM_FP16, 8, 6, 0)])
 def test_grouped_icd_reaches_converged_cost(ctx, converged_cfg1_small, weights, wpv, stage, pairs):
     """FP16 with the streamed (one warp) or 4/8-warp kernels reads the
     matrix as entry pairs (pairs 0) or as single entries (pairs -1)."""
@@ -244,7 +245,7 @@ def test_entry_pairs_match_single_entries(ctx, converged_cfg1_small, wpv):
     assert info.nnz / 2 <= info.n_pairs <= 0.75 * info.nnz, (info.n_pairs, info.nnz)
 
 
-@pytest.mark.parametrize("stage", [4, 5])
+@pytest.mark.parametrize("stage", [4, 5, 6])
 @pytest.mark.parametrize("case", ["cfg1_small", "small_ffs"])
 def test_bulk_staged_kernel_matches_cta_pairs(ctx, converged_cfg1_small, converged_small_ffs, case, stage):
     """One update in flight: the kernel whose entry pairs arrive in shared
@@ -328,7 +329,8 @@ def converged_small_ffs(ctx, tmp_path_factory):
     return rp, data, ssm, x_ref, cost_ref
 
 
-@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1), (C.SSM_FP16, 3), (C.SSM_FP16, 5)])
+@pytest.mark.parametrize("weights,stage", [(C.SSM_FP32, 0), (C.SSM_FP16, 1), (C.SSM_FP16, 3), (C.SSM_FP16, 5),
+                                           (C.SSM_FP16, 6)])
 def test_grouped_edge_preserving_reaches_converged_cost(ctx, converged_small_ffs, weights, stage):
     rp, data, ssm, x_ref, cost_ref = converged_small_ffs
     rc = C.Recon(rp, data.slice_indices, ctx)
