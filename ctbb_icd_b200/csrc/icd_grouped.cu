@@ -67,7 +67,8 @@ struct GParams {
     double relax;  // step scale applied to the exact 1-D update before the positivity clamp
     double cvx, cvy, vx, vy, fov_limit;
     int stack_align;  // CTA kernels: sweep from the slice stack's common data view
-    int l2_hints;     // CTA kernels: matrix loads evict-first, e gathers evict-last
+    int l2_hints;     // CTA kernels: matrix loads evict-first, e gathers evict-last;
+                      // bulk kernels (stage_column 4/5): the column copy evict-first
 };
 
 __device__ __forceinline__ float warp_sum(float v) {
@@ -877,6 +878,15 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  "l"(src), "r"(bytes), "r"(bar)
                  : "memory");
 }
+// The same copy with an L2 eviction policy (createpolicy) for the source lines.
+__device__ __forceinline__ void bulk_g2s_hint(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar,
+                                              uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1], %2, [%3], %4;" ::"r"(
+            dst),
+        "l"(src), "r"(bytes), "r"(bar), "l"(pol)
+        : "memory");
+}
 
 // Thread 0: take the next work item and start the copy of its pairs into
 // the stage at `dst` (bytes counted on `bar`). Pairs [b0, e1) are copied with
@@ -924,7 +934,15 @@ __device__ __forceinline__ void bulk_issue(const GParams& P, const uint32_t* __r
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     bulk_mbar_expect_tx(bar, bytes);
     const char* src = reinterpret_cast<const char*>(pairs + b0);
-    for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
+    if (P.l2_hints) {
+        // The column is read once per update and kept in shared memory for
+        // the scatter: mark its L2 lines first to go, leaving L2 to e.
+        const uint64_t pol = l2_drop();
+        for (uint32_t o = 0; o < bytes; o += kBulkChunk)
+            bulk_g2s_hint(dst + o, src + o, min(kBulkChunk, bytes - o), bar, pol);
+    } else {
+        for (uint32_t o = 0; o < bytes; o += kBulkChunk) bulk_g2s(dst + o, src + o, min(kBulkChunk, bytes - o), bar);
+    }
 }
 
 template <int STAGES>

@@ -330,7 +330,9 @@ typedef struct ctbb_icd_opts {
                                  from its start                                   */
     int32_t l2_hints;         /* grouped, 4 or 8 warps per voxel: 1 marks the matrix
                                  loads (read once per update) evict-first and the
-                                 e gathers evict-last in L2; 0 leaves both normal */
+                                 e gathers evict-last in L2; with stage_column 4/5
+                                 1 marks the column's bulk copy evict-first; 0
+                                 leaves them normal                               */
 } ctbb_icd_opts;
 
 /*
