@@ -259,6 +259,7 @@ def run_ours(args, rank, world, dist):
                 "ssm_nnz": int(info.nnz), "ssm_bytes": int(info.bytes_device),
                 "ssm_build_ms": round(info.build_ms, 2), "inrange_entries_per_iter": entries,
                 "scattered_entries_per_iter": scattered, "stage_column": int(opts.stage_column),
+                "l2_hints": int(opts.l2_hints),
                 "matrix_read_as": (f"{n_pairs} entry pairs (8 B each)" if uses_pairs
                                    else f"entries ({4 + w_bytes} B each)"),
                 "warps_in_flight": opts.warps_in_flight or "auto", "warps_per_voxel": max(1, opts.warps_per_voxel),
