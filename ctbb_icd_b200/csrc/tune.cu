@@ -89,7 +89,11 @@ extern "C" ctbb_status ctbb_gpu_recon_autotune(ctbb_recon* rc, const ctbb_ssm* s
     cands.push_back({8, 4 * sms * 8, 8, 0, 0, 0});
     // One update per CTA of 8 warps with the entry pairs bulk-copied into
     // shared memory: one stage (four CTAs per SM) or two (three per SM).
-    if (o.weights == CTBB_SSM_FP16) {
+    // These kernels read entry pairs only: build them now (outside any
+    // stream capture) and skip the kernels for a matrix whose detector-row
+    // runs do not pair up (z flying focal spot), which keeps none.
+    if (o.weights == CTBB_SSM_FP16 && status == CTBB_OK) status = ssm_build_pairs(const_cast<ctbb_ssm*>(ssm));
+    if (o.weights == CTBB_SSM_FP16 && status == CTBB_OK && ssm->d_pairs) {
         cands.push_back({8, 4 * sms * 8, 8, 0, 4, 0});
         cands.push_back({8, 3 * sms * 8, 8, 0, 5, 0});
         // The one-stage kernel with the next item claimed during the

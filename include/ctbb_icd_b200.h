@@ -493,7 +493,8 @@ ctbb_status ctbb_gpu_rotate_device_noalloc(ctbb_ctx* ctx, const ctbb_geom_c* geo
  * in flight and the default tile edge for that concurrency (half of it too
  * at the default); 4 warps per voxel with four or eight updates per SM and
  * 8 warps per voxel with four (these read entry pairs with FP16 weights);
- * with FP16 weights, the bulk-staged kernels (stage_column 4, 5 and 6).
+ * with FP16 weights, the bulk-staged kernels (stage_column 4, 5 and 6),
+ * unless the matrix keeps no entry pairs (z flying focal spot).
  * Every launch keeps at most one cell rank of the visiting order (about
  * n / T^2 updates for tile edge T) in flight, so no two in-plane neighbours
  * of a slice are ever updated together; trials report the effective warps

@@ -210,6 +210,26 @@ def test_autotune_leaves_iterate_and_picks_a_candidate(ctx):
     assert st.iterations == 2
 
 
+@pytest.mark.parametrize("name", ["tiny_zffs", "small_ffs"])
+def test_autotune_fp16_probes_bulk_kernels_only_with_entry_pairs(ctx, name):
+    """With FP16 weights the tuner probes the bulk-staged kernels, which read
+    entry pairs, only when the matrix keeps pairs: a z flying focal spot
+    matrix whose rows do not pair up still tunes (over the other kernels)."""
+    scan = L.make_scan(ctx, name, seed=3, weights=C.SSM_FP16)
+    opts = C.icd_opts(mode=C.ICD_GROUPED, weights=C.SSM_FP16)
+    scan.rc.iterate(scan.ssm, 1, opts)
+    best, trials = scan.rc.autotune(scan.ssm, opts, probe_iters=1)
+    stages = {t["stage_column"] for t in trials}
+    if scan.ssm.info().n_pairs == 0:
+        assert not stages & {4, 5, 6}, stages
+    else:
+        assert {4, 5, 6} <= stages, stages
+    st = scan.rc.iterate(scan.ssm, 1, best)
+    assert st.iterations == 1 and np.isfinite(scan.rc.volume()).all()
+    scan.rc.free()
+    scan.ssm.free()
+
+
 def test_trained_warm_start_beats_plain_icd(ctx):
     """The committed network on a scan it was not trained on (seed 905 of the
     training geometry): after the warm start and the same number of full
