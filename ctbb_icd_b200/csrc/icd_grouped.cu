@@ -85,17 +85,6 @@ __device__ __forceinline__ double sum8(double v) {
     return __shfl_sync(0xffffffffu, v, 0);
 }
 
-template <class WT>
-__device__ __forceinline__ float ldw(const WT* w, int64_t m);
-template <>
-__device__ __forceinline__ float ldw<float>(const float* w, int64_t m) {
-    return __ldg(w + m);
-}
-template <>
-__device__ __forceinline__ float ldw<__half>(const __half* w, int64_t m) {
-    return __half2float(__ldg(w + m));
-}
-
 // L2 eviction policies: a voxel update reads its matrix entries twice (gather,
 // then scatter); the gather's loads ask L2 to keep the lines, the scatter's
 // to drop them first.
