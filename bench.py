@@ -874,7 +874,9 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     dist = None
-    if world > 1:
+    # The reference arm is rank 0's CPU work alone: no process group, and the
+    # other ranks exit at once without touching a GPU.
+    if world > 1 and args.impl != "reference":
         import datetime
 
         import torch
