@@ -80,7 +80,9 @@ def test_sequential_icd_matches_reference_at_bench_size(bench_fixture, ctx):
 @pytest.mark.parametrize("name", ["cfg2", "cfg2_center"])
 def test_ssm_full_geometry_sampled_columns_match_oracle(name, ctx, tmp_path):
     _, rp = W.materialise(name, str(tmp_path), raw=False)
+    C.slice_tables(rp)  # load_raw's tables set table_direction: the source advances in z
     g = rp.geom
+    assert g.table_direction == -1
     ssm = C.Ssm.generate(rp, ctx, C.SSM_FP32)
     nx, ncol = int(g.nx), int(g.nx * g.ny)
     nvsm = int(g.num_views_for_system_matrix)
