@@ -245,6 +245,12 @@ typedef struct ctbb_ssm_info {
  * Replaces generate_system_matrix (src/generate_system_matrix.cpp:54-209) and
  * generate_system_matrix_ffs (src/generate_system_matrix_ffs.cpp:60-239);
  * the on-disk matrix.bin round trip (:212-303) becomes an HBM-resident matrix.
+ * As in the reference's flow (load_raw before generate_system_matrix,
+ * main.cpp:92, 101-109), geom must have passed ctbb_slice_tables: it sets
+ * table_direction, whose sign moves the source along z from view to view
+ * (generate_system_matrix.cpp:100). With table_direction 0, as
+ * ctbb_configure_recon_params leaves it, the source stays at z = 0 and the
+ * matrix models a circular scan.
  */
 ctbb_status ctbb_gpu_generate_ssm(ctbb_ctx* ctx, const ctbb_geom_c* geom, int32_t weights,
                                   ctbb_ssm** out);
