@@ -30,22 +30,31 @@ import oracle_util as O  # noqa: E402
 
 def view_tables(g, ffs):
     """Per-view source, frame and flying-focal-spot deflection (ssm.cu
-    host_tables; generate_system_matrix.cpp:85-100, _ffs.cpp:134, 253-259).
-    In-plane deflection only: the z flying focal spot has its own rows."""
+    host_tables; generate_system_matrix.cpp:85-100, generate_system_matrix_ffs
+    .cpp:66-67, 134, 242-290: in-plane +/-da e_u by view parity, z -/+dr e_w
+    -/+dr tan(anode_angle) e_z with the angle in degrees passed to tan, or the
+    four combinations of both)."""
     nvsm = int(g.num_views_for_system_matrix)
     i = np.arange(nvsm, dtype=np.float64)
+    k = np.arange(nvsm)
     ta = (i - 0.5 * nvsm) * g.tube_angle_increment
     ew0, ew1, eu0, eu1 = np.cos(ta), np.sin(ta), -np.sin(ta), np.cos(ta)
     zs = g.table_direction * (i - 0.5 * nvsm) * g.tube_z_increment
     SDD, R = g.source_detector_distance, g.focal_spot_radius
-    off0 = np.zeros(nvsm)
-    off1 = np.zeros(nvsm)
-    if ffs:
-        da = SDD * R * np.sin(g.fan_angle_increment) / (4.0 * (SDD - R))
-        s = np.where(np.arange(nvsm) % 2 == 0, da, -da)
-        off0, off1 = s * eu0, s * eu1
-    return dict(src0=R * ew0 + off0, src1=R * ew1 + off1, src2=zs, ew0=ew0, ew1=ew1, eu0=eu0, eu1=eu1,
-                off0=off0, off1=off1, off2=np.zeros(nvsm))
+    da = SDD * R * np.sin(g.fan_angle_increment) / (4.0 * (SDD - R))
+    dr = SDD * g.CollSlicewidth / (4.0 * (SDD - R) * np.tan(g.anode_angle * 3.14159265359 / 180.0))
+    a = np.zeros(nvsm)  # in-plane deflection along e_u
+    r = np.zeros(nvsm)  # z-spot deflection along e_w (and r tan(anode_angle) along e_z)
+    if ffs and not g.Zffs:
+        a = np.where(k % 2 == 0, da, -da)
+    elif ffs and not g.Phiffs:
+        r = np.where(k % 2 == 0, -dr, dr)
+    elif ffs:
+        r = np.where(k % 4 < 2, -dr, dr)
+        a = np.where(k % 2 == 0, -da, da)
+    off0, off1, off2 = r * ew0 + a * eu0, r * ew1 + a * eu1, r * np.tan(g.anode_angle)
+    return dict(src0=R * ew0 + off0, src1=R * ew1 + off1, src2=zs + off2, ew0=ew0, ew1=ew1, eu0=eu0, eu1=eu1,
+                off0=off0, off1=off1, off2=off2)
 
 
 def candidate_slack(g, ffs, col, v, ch, row):
@@ -92,13 +101,24 @@ def candidate_slack(g, ffs, col, v, ch, row):
     return np.minimum.reduce([ch - ch_lo, ch_hi - ch, row - r_lo, r_hi - row])
 
 
-@pytest.mark.parametrize("name", ["cfg2", "cfg1"])
-def test_candidate_bounds_contain_every_reference_entry_at_bench_size(tmp_path, name):
-    _, rp = W.materialise(name, str(tmp_path), raw=False)
+# The benchmark geometries, and cfg2's scanner with the z flying focal spot
+# (32 rows per projection, setup.cpp:225) alone and with the in-plane one.
+CASES = {
+    "cfg2": ("cfg2", None),
+    "cfg1": ("cfg1", None),
+    "cfg2_zffs": ("cfg2", {"Zffs": 1, "Phiffs": 0, "center_row": 15.5}),
+    "cfg2_zphiffs": ("cfg2", {"Zffs": 1, "Phiffs": 1, "center_row": 15.5, "Readings": 18432}),
+}
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_candidate_bounds_contain_every_reference_entry_at_bench_size(tmp_path, case):
+    name, overrides = CASES[case]
+    _, rp = W.materialise(name, str(tmp_path), raw=False, overrides=overrides)
     C.slice_tables(rp)  # load_raw's tables set table_direction (setup.cpp:275)
     g = rp.geom
     assert g.table_direction == -1
-    ffs = bool(g.Phiffs)
+    ffs = bool(g.Phiffs or g.Zffs)
     nx = int(g.num_voxels_x)
     ncol = nx * int(g.num_voxels_y)
     nvsm = int(g.num_views_for_system_matrix)
@@ -116,7 +136,7 @@ def test_candidate_bounds_contain_every_reference_entry_at_bench_size(tmp_path, 
         v, rem = q // per_view, q % per_view
         ch, row = rem // int(g.Nrows_projection), rem % int(g.Nrows_projection)
         slack = candidate_slack(g, ffs, int(c), v, ch, row)
-        assert slack.min() >= 0, (name, int(c), int(slack.min()), int(np.count_nonzero(slack < 0)))
+        assert slack.min() >= 0, (case, int(c), int(slack.min()), int(np.count_nonzero(slack < 0)))
         n_checked += q.size
     # Measured: every entry sits at least 3 channels inside its candidate
     # range and, away from the detector's first and last rows (where the
