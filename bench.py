@@ -41,6 +41,7 @@ WORKLOAD = "cfg2"
 WORKLOAD_TEXT = ("grouped ICD, 512x512x64 @ 0.6 mm, 30 cm FOV, 736 ch x 64 rows, in-plane FFS, "
                  "2304 views/turn, 4 turns (9216 views), edge-preserving (delta 9.6e-4, lambda 0.1)")
 HBM_FALLBACK_GBS = 6650.0
+HBM_NOMINAL_GBS = 8000.0  # B200 HBM3e nominal, for context beside the measured copy peak
 
 
 def measured_peak():
@@ -275,6 +276,8 @@ def run_ours(args, rank, world, dist):
                 "kernel": kernel,
                 "algorithmic_bytes_per_launch": b_iter,
                 "kernel_ms_per_launch": kernel_ms_per_launch, "peak_source": peak_kind,
+                "frac_of_nominal": achieved / HBM_NOMINAL_GBS, "nominal_peak": HBM_NOMINAL_GBS,
+                "traffic_gbs": None if traffic is None else traffic / (kernel_ms_per_launch / 1e3) / 1e9,
             },
             "gpu_launches": int(args.steps),
             "clocks": clocks.summary(),
